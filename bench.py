@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Graph500 plain direction-optimizing BFS on B200: harmonic-mean GTEPS.
+
+One step = BFS from every one of the NROOTS find_roots roots (default 64,
+REAL_BENCHMARK) of a Kronecker SCALE 22 / edgefactor 16 graph built on the GPU
+with VERTEX_REORDERING 2.  Each BFS is timed on the device with CUDA events on
+the library's stream, with L2 flushed before every root (outside the event
+pair).  value = traversed edges (validate.hpp edge_visit_count) / BFS time,
+which for this graph equals the Graph500 harmonic mean (every root reaches the
+same component).  e2e = the same through the reference-facing call
+run_bfs(root, pred) with pred in pinned HOST memory, the device-to-host copy of
+pred inside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 (torchrun) runs N independent replicas (one per GPU); value is the sum
+of their edges over the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GTEPS (harmonic mean, 1×B200) plain vs batched MS-BFS; serving p50/p99 latency"
+UNIT = "GTEPS"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--edgefactor", type=int, default=16)
+    ap.add_argument("--roots", type=int, default=64)
+    ap.add_argument("--reorder", type=int, default=2)
+    ap.add_argument("--alpha", type=float, default=2000.0)
+    ap.add_argument("--beta", type=float, default=8.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-roots", type=int, default=8, help="roots in the bounded CPU-baseline sample")
+    ap.add_argument("--ref-roots-per-step", type=int, default=4)
+    return ap.parse_args()
+
+
+def workload(a) -> dict:
+    return {"workload": f"plain direction-optimizing BFS, Kronecker SCALE {a.scale} edgefactor {a.edgefactor}, "
+                        f"VERTEX_REORDERING {a.reorder}, {a.roots} roots per step",
+            "scale": a.scale, "edgefactor": a.edgefactor, "roots_per_step": a.roots,
+            "vertex_reordering": a.reorder, "alpha": a.alpha, "beta": a.beta,
+            "l2": "flushed (256 MiB write) before every root, outside the timed events",
+            "parallelism": f"replicas x{a.gpus}"}
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append({"sm": float(parts[1]), "max": float(parts[2]), "active": parts[4],
+                             "hw": parts[5], "hwt": parts[6], "swt": parts[7], "pcap": parts[8]})
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        reasons = set()
+        for r in rows:
+            for k, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
+                            ("pcap", "sw_power_cap")):
+                if r[k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["max"] for r in rows),
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+# --------------------------------------------------------------------------- CPU baseline
+def run_ref_bench(scale, ef, nroots, warmup, steps, per_step, reorder):
+    exe = os.path.join(ROOT, "oracle", "_ref", f"ref_bench_vr{reorder}")
+    if not os.path.exists(exe):
+        return None, f"{exe} not built"
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    env.pop("NO_AFFINITY", None)
+    r = subprocess.run([exe, str(scale), str(ef), str(nroots), str(warmup), str(steps), str(per_step)],
+                       capture_output=True, text=True, env=env)
+    if r.returncode != 0:
+        return None, f"ref_bench exit {r.returncode}: {r.stderr.strip().splitlines()[-1:]}"
+    rec = json.loads(r.stdout.strip().splitlines()[-1])
+    rec["cores"] = cores
+    return rec, None
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    rec, err = run_ref_bench(a.scale, a.edgefactor, min(a.roots, 64), a.warmup, a.steps, a.ref_roots_per_step,
+                             a.reorder)
+    if rec is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    runs = rec["runs"]
+    t = sum(x[2] for x in runs)
+    e = sum(x[3] for x in runs)
+    hm = 1.0 / (sum(x[2] / x[3] for x in runs) / len(runs))
+    value = e / t / 1e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1000.0 * t / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic (Graph500 Kronecker generator, seeds 2/3)",
+            "impl": "reference", "config": dict(workload(a), roots_per_step=a.ref_roots_per_step,
+                                                 parallelism="1 process, OpenMP"),
+            "harmonic_mean_gteps": hm / 1e9,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": rec["cores"], "kind": "reference",
+                             "sample": f"{len(runs)} BFS runs ({a.ref_roots_per_step} roots/step) of the "
+                                       f"reference run_bfs at SCALE {a.scale}, {cpu_model()}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "generation_s": rec["generation_s"], "construction_s": rec["construction_s"]}
+    print(json.dumps(line))
+
+
+# --------------------------------------------------------------------------- our arm
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def bytes_model(levels, pred_size, nlv):
+    """Algorithmic bytes of one BFS: 8 B per pred entry, and per level
+    TD: 32 B per frontier vertex (offsets) + 32 B per adjacency sector + 32 B per discovered vertex;
+    BU: the visited bitmap (nlv/8 B) + 8 B per scanned vertex + 32 B per adjacency sector."""
+    td = bu = 0
+    for l in levels:
+        if l["direction"] == 1:
+            td += 32 * l["frontier"] + 32 * l["edge_sectors"] + 32 * l["discovered"]
+        else:
+            bu += nlv // 8 + 8 * l["scanned"] + 32 * l["edge_sectors"]
+    return 8 * pred_size, td, bu
+
+
+def our_arm(a):
+    import torch
+
+    import graph500_b200 as g5
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def reduce_max(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def reduce_sum(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        return float(t.item())
+
+    bfs = g5.BfsOnGPU(device=local, reorder_mode=a.reorder)
+    t0 = time.time()
+    bfs.construct(g5.EdgeList(None, a.scale, a.edgefactor))
+    gen_s, build_s = bfs.graph_.timings()
+    info = bfs.graph_.info
+    bfs.prepare_bfs(a.alpha, a.beta, count_edges=True)
+    roots = g5.find_roots(bfs.graph_, a.roots)
+    pred_dev = torch.empty(info.pred_size, dtype=torch.int64, device="cuda")
+
+    # untimed: validate every root, record the per-level counts of the bytes model
+    nedge, model = [], []
+    for r in roots:
+        bfs.run_bfs(int(r), pred_dev)
+        ok, evc, rep = g5.validate_bfs_result(bfs.graph_, int(r), pred_dev)
+        if not ok:
+            raise SystemExit(f"validation failed for root {r}: {rep}")
+        nedge.append(evc)
+        model.append(bytes_model(bfs.level_stats(), info.pred_size, info.num_local_verts))
+    bfs.set_params(a.alpha, a.beta, count_edges=False)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step(record: dict | None):
+        for i, r in enumerate(roots):
+            flush.zero_()
+            torch.cuda.synchronize()
+            st = bfs.run_bfs(int(r), pred_dev)
+            if record is not None:
+                record["t"].append(st.device_ms)
+                record["e"].append(nedge[i])
+                record["launches"] += st.kernel_launches
+                for l in bfs.level_stats():
+                    key = "td" if l["direction"] == 1 else "bu"
+                    record[key + "_ms"] += l["device_ms"]
+                    record[key + "_launches"] += 1
+                pb, tdb, bub = model[i]
+                record["td_bytes"] += tdb
+                record["bu_bytes"] += bub
+                record["pred_bytes"] += pb
+
+    for _ in range(a.warmup):
+        step(None)
+    rec = {"t": [], "e": [], "launches": 0, "td_ms": 0.0, "bu_ms": 0.0, "td_launches": 0, "bu_launches": 0,
+           "td_bytes": 0, "bu_bytes": 0, "pred_bytes": 0}
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    for _ in range(a.steps):
+        step(rec)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    t_rank = sum(rec["t"]) / 1000.0
+    t_max = reduce_max(t_rank)
+    e_all = reduce_sum(float(sum(rec["e"])))
+    value = e_all / t_max / 1e9
+    hm = 1.0 / (sum(t / 1000.0 / e for t, e in zip(rec["t"], rec["e"])) / len(rec["t"])) / 1e9
+
+    # e2e: run_bfs into pinned host memory, the D2H copy of pred inside the wall-clock time
+    hp = __import__("ctypes").c_void_p()
+    g5.check(g5.lib().g500_host_alloc(8 * info.pred_size, __import__("ctypes").byref(hp)))
+    host_pred = np.ctypeslib.as_array((__import__("ctypes").c_int64 * info.pred_size).from_address(hp.value))
+    for r in roots[:4]:
+        bfs.run_bfs(int(r), host_pred)
+    barrier()
+    e2e_t = 0.0
+    for _ in range(a.steps):
+        for r in roots:
+            flush.zero_()
+            torch.cuda.synchronize()
+            w0 = time.perf_counter()
+            bfs.run_bfs(int(r), host_pred)
+            e2e_t += time.perf_counter() - w0
+    barrier()
+    e2e_max = reduce_max(e2e_t)
+    e2e_value = e_all / e2e_max / 1e9
+    g5.check(g5.lib().g500_host_free(hp))
+
+    if rank != 0:
+        bfs.close()
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    peak, peak_kind = load_peaks()
+    dom = "bu" if rec["bu_ms"] >= rec["td_ms"] else "td"
+    dom_bytes = rec[dom + "_bytes"] / max(rec[dom + "_launches"], 1)
+    dom_ms = rec[dom + "_ms"] / max(rec[dom + "_launches"], 1)
+    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9 if dom_ms > 0 else 0.0
+    whole = (rec["td_bytes"] + rec["bu_bytes"] + rec["pred_bytes"]) / (sum(rec["t"]) / 1000.0) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1000.0 * t_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic (Graph500 Kronecker generator, seeds 2/3, generated on the GPU)",
+        "config": workload(a),
+        "harmonic_mean_gteps": hm,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * len(roots),
+                "d2h_bytes_per_step": 8 * info.pred_size * len(roots)},
+        "gpu_launches": rec["launches"],
+        "roofline": {"bound": "hbm", "kernel": f"{dom}_kernel", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "whole_bfs_achieved": whole, "whole_bfs_frac": whole / peak,
+                     "bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
+                     "level_ms": {"td": rec["td_ms"] / len(rec["t"]), "bu": rec["bu_ms"] / len(rec["t"])}},
+        "clocks": clocks,
+        "graph": {"num_global_verts": info.num_global_verts, "num_global_edges": info.num_global_edges,
+                  "pred_size": info.pred_size, "nedge_per_root": int(statistics.median(nedge)),
+                  "generation_s": gen_s, "construction_s": build_s, "setup_wall_s": time.time() - t0},
+    }
+    if world == 1 and not a.no_cpu_baseline:
+        crec, err = run_ref_bench(a.scale, a.edgefactor, a.cpu_roots, 0, 1, a.cpu_roots, a.reorder)
+        if crec is not None:
+            runs = crec["runs"]
+            cv = sum(x[3] for x in runs) / sum(x[2] for x in runs) / 1e9
+            line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": crec["cores"], "kind": "reference",
+                                    "sample": f"{len(runs)} roots of the reference run_bfs at SCALE {a.scale} "
+                                              f"(same graph), OMP {crec['cores']} threads, {cpu_model()}"}
+        else:
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": err}
+    print(json.dumps(line))
+    bfs.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse_args()
+    if a.impl == "reference":
+        reference_arm(a)
+    else:
+        our_arm(a)
+
+
+if __name__ == "__main__":
+    main()

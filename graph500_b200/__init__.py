@@ -1,0 +1,365 @@
+"""graph500_b200 -- B200-native Graph500 BFS behind the reference's BfsBase interface.
+
+Python mirror of the suzumura/graph500 driver-facing API (mpi/main.cc and
+mpi/bfs.hpp), bound to libg500.so through its C ABI (include/g500.h):
+
+    edge_list = generate_graph_spec2010(SCALE, edgefactor)      # benchmark_helper.hpp:308
+    bfs = BfsOnGPU(); bfs.construct(edge_list)                   # bfs.hpp:102
+    roots = find_roots(bfs.graph_, 64)                           # benchmark_helper.hpp:475
+    bfs.prepare_bfs()                                            # bfs.hpp:115
+    bfs.run_bfs(root, pred)                                      # bfs.hpp:120
+    ok, nedge = validate_bfs_result(edge_list, max_used_vertex(bfs.graph_) + 1,
+                                    bfs.graph_.pred_size(), root, pred)   # validate.hpp:1008
+    bfs.end_bfs()                                                # bfs.hpp:126
+
+There is no CPU fallback: every call runs the CUDA library, and importing a
+function whose library is missing raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libg500.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "g500.h")
+USERSEED1, USERSEED2 = 2, 3  # mpi/parameters.h:190-191
+EDGE_DTYPE = np.dtype([("v0_low", "<u4"), ("v1_low", "<u4"), ("high", "<u4")])
+
+G500_OK, G500_E_INVAL, G500_E_NOMEM, G500_E_DEVICE, G500_E_TIMEOUT, G500_E_RANGE, G500_E_STATE = range(7)
+
+
+class G500Error(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[g500 status {code}] {msg}")
+        self.code = code
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [("log_orig_global_verts", C.c_int64), ("pred_size", C.c_int64), ("num_local_verts", C.c_int64),
+                ("num_global_verts", C.c_int64), ("num_global_edges", C.c_int64), ("max_used_vertex", C.c_int64),
+                ("num_input_edges", C.c_int64), ("device_bytes", C.c_int64), ("reorder_mode", C.c_int32),
+                ("device", C.c_int32)]
+
+
+class LevelStats(C.Structure):
+    _fields_ = [("direction", C.c_int32), ("level", C.c_int32), ("frontier", C.c_int64),
+                ("discovered", C.c_int64), ("scanned", C.c_int64), ("edge_sectors", C.c_int64),
+                ("edges_examined", C.c_int64), ("device_ms", C.c_double)]
+
+
+class BfsStats(C.Structure):
+    _fields_ = [("device_ms", C.c_double), ("host_ms", C.c_double), ("reached", C.c_int64), ("nedge", C.c_int64),
+                ("num_levels", C.c_int32), ("td_levels", C.c_int32), ("bu_levels", C.c_int32),
+                ("kernel_launches", C.c_int32)]
+
+
+class ValidateReport(C.Structure):
+    _fields_ = [("range_errors", C.c_int64), ("root_errors", C.c_int64), ("self_parent_errors", C.c_int64),
+                ("depth_errors", C.c_int64), ("edge_errors", C.c_int64),
+                ("missing_parent_edge_errors", C.c_int64)]
+
+
+_lib = None
+
+
+def header_functions() -> list[str]:
+    """Names of the functions include/g500.h declares."""
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\*?\s+\*?(g500_\w+)\s*\(", text, re.M)))
+
+
+def lib() -> C.CDLL:
+    """Load libg500.so (raise if it was not built: there is no fallback path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with `python -m graph500_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P, i64, u64, i32 = C.c_void_p, C.c_int64, C.c_uint64, C.c_int
+    sig = {
+        "g500_last_error": ([], C.c_char_p),
+        "g500_abi_version": ([], i32),
+        "g500_host_alloc": ([u64, C.POINTER(P)], i32),
+        "g500_host_free": ([P], i32),
+        "g500_scramble_values": ([i32, u64, u64, C.POINTER(u64), C.POINTER(u64)], i32),
+        "g500_gen_edges": ([i32, i32, u64, u64, i64, i64, P, i32, P], i32),
+        "g500_graph_build": ([P, i64, i32, i32, i32, i32, C.POINTER(P)], i32),
+        "g500_graph_generate": ([i32, i32, u64, u64, i32, i32, C.POINTER(P)], i32),
+        "g500_graph_info_get": ([P, C.POINTER(GraphInfo)], i32),
+        "g500_graph_has_edge": ([P, i64, C.POINTER(i32)], i32),
+        "g500_graph_find_roots": ([P, i32, u64, u64, P, C.POINTER(i32)], i32),
+        "g500_graph_edges": ([P, C.POINTER(P), C.POINTER(i64)], i32),
+        "g500_graph_copy_csr": ([P, P, P, P], i32),
+        "g500_graph_timings": ([P, C.POINTER(C.c_double), C.POINTER(C.c_double)], i32),
+        "g500_graph_destroy": ([P], i32),
+        "g500_bfs_create": ([P, C.POINTER(P)], i32),
+        "g500_bfs_set_params": ([P, C.c_double, C.c_double, i32], i32),
+        "g500_bfs_set_stream": ([P, P], i32),
+        "g500_bfs_run": ([P, i64, P, i32, C.POINTER(BfsStats)], i32),
+        "g500_bfs_level_stats": ([P, P, i32, C.POINTER(i32)], i32),
+        "g500_bfs_device_pred": ([P, C.POINTER(P)], i32),
+        "g500_bfs_destroy": ([P], i32),
+        "g500_validate": ([P, P, i64, i32, i64, P, i32, C.POINTER(i64), C.POINTER(i32), C.POINTER(ValidateReport)],
+                          i32),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def check(status: int) -> None:
+    if status != G500_OK:
+        raise G500Error(status, lib().g500_last_error().decode(errors="replace"))
+
+
+def _ptr(obj) -> tuple[int, bool]:
+    """(address, on_device) of a numpy array or a CUDA array (e.g. a torch tensor)."""
+    if isinstance(obj, np.ndarray):
+        if not obj.flags.c_contiguous:
+            raise ValueError("array must be C-contiguous")
+        return obj.ctypes.data, False
+    cai = getattr(obj, "__cuda_array_interface__", None)
+    if cai is not None:
+        return int(cai["data"][0]), True
+    raise TypeError(f"unsupported buffer type {type(obj)!r}")
+
+
+# ---------------------------------------------------------------------------
+# (a) generation
+# ---------------------------------------------------------------------------
+class EdgeList:
+    """The generated edge list (EdgeListStorage, generator/graph_generator.hpp:35-319).
+
+    Host edges are a numpy array of 12-byte packed edges; a device-resident
+    list belongs to a graph built by ``generate_graph_spec2010(..., device=True)``.
+    """
+
+    def __init__(self, edges: np.ndarray | None = None, scale: int | None = None, edgefactor: int = 16):
+        self.edges = edges
+        self.scale = scale
+        self.edgefactor = edgefactor
+
+    def num_local_edges(self) -> int:
+        return len(self.edges) if self.edges is not None else (1 << self.scale) * self.edgefactor
+
+
+def generate_edges(scale: int, edgefactor: int = 16, start: int = 0, end: int | None = None,
+                   seed1: int = USERSEED1, seed2: int = USERSEED2, out=None):
+    """Edges [start, end) of the spec-2010 Kronecker graph, generated on the GPU."""
+    if end is None:
+        end = (1 << scale) * edgefactor
+    if out is None:
+        out = np.zeros(end - start, dtype=EDGE_DTYPE)
+    ptr, dev = _ptr(out)
+    check(lib().g500_gen_edges(scale, edgefactor, seed1, seed2, start, end, ptr, int(dev), None))
+    return out
+
+
+def generate_graph_spec2010(scale: int, edgefactor: int = 16) -> EdgeList:
+    """generate_graph_spec2010 (mpi/benchmark_helper.hpp:308-314) into host memory."""
+    return EdgeList(generate_edges(scale, edgefactor), scale, edgefactor)
+
+
+def scramble_values(scale: int, seed1: int = USERSEED1, seed2: int = USERSEED2) -> tuple[int, int]:
+    a, b = C.c_uint64(), C.c_uint64()
+    check(lib().g500_scramble_values(scale, seed1, seed2, C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+# ---------------------------------------------------------------------------
+# (b) construction
+# ---------------------------------------------------------------------------
+class Graph2DCSR:
+    """Device-resident graph (mpi/graph_constructor.hpp:24-143) for one GPU."""
+
+    def __init__(self, handle: int):
+        self.h = C.c_void_p(handle)
+        info = GraphInfo()
+        check(lib().g500_graph_info_get(self.h, C.byref(info)))
+        self.info = info
+        self.log_orig_global_verts_ = info.log_orig_global_verts
+        self.num_local_verts_ = info.num_local_verts
+        self.num_global_verts_ = info.num_global_verts
+        self.num_global_edges_ = info.num_global_edges
+        self.reorder_mode = info.reorder_mode
+
+    @classmethod
+    def build(cls, edges: np.ndarray, reorder_mode: int = 2, keep_edges: bool = True, device: int = 0):
+        ptr, dev = _ptr(edges)
+        h = C.c_void_p()
+        check(lib().g500_graph_build(ptr, len(edges), int(dev), reorder_mode, int(keep_edges), device,
+                                     C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def generate(cls, scale: int, edgefactor: int = 16, reorder_mode: int = 2, device: int = 0,
+                 seed1: int = USERSEED1, seed2: int = USERSEED2):
+        h = C.c_void_p()
+        check(lib().g500_graph_generate(scale, edgefactor, seed1, seed2, reorder_mode, device, C.byref(h)))
+        return cls(h.value)
+
+    def pred_size(self) -> int:
+        return self.info.pred_size
+
+    def log_orig_global_verts(self) -> int:
+        return self.info.log_orig_global_verts
+
+    def has_edge(self, v: int) -> bool:
+        out = C.c_int()
+        check(lib().g500_graph_has_edge(self.h, v, C.byref(out)))
+        return bool(out.value)
+
+    def timings(self) -> tuple[float, float]:
+        a, b = C.c_double(), C.c_double()
+        check(lib().g500_graph_timings(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def device_edges(self) -> tuple[int, int]:
+        p, m = C.c_void_p(), C.c_int64()
+        check(lib().g500_graph_edges(self.h, C.byref(p), C.byref(m)))
+        return (p.value or 0), m.value
+
+    def copy_csr(self) -> dict:
+        nlv, nge, nolv = self.info.num_local_verts, self.info.num_global_edges, self.info.pred_size
+        offsets = np.zeros(nlv + 1, np.uint64)
+        cols = np.zeros(max(nge, 1), np.uint32)
+        rmap = np.zeros(nolv, np.uint32)
+        check(lib().g500_graph_copy_csr(self.h, offsets.ctypes.data, cols.ctypes.data, rmap.ctypes.data))
+        return {"offsets": offsets, "cols": cols[:nge], "reorder_map": rmap}
+
+    def close(self) -> None:
+        if self.h is not None and self.h.value:
+            check(lib().g500_graph_destroy(self.h))
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def find_roots(graph: Graph2DCSR, num_roots: int, seed1: int = USERSEED1, seed2: int = USERSEED2) -> np.ndarray:
+    """find_roots (mpi/benchmark_helper.hpp:475-508)."""
+    out = np.zeros(num_roots, np.int64)
+    n = C.c_int()
+    check(lib().g500_graph_find_roots(graph.h, num_roots, seed1, seed2, out.ctypes.data, C.byref(n)))
+    return out[:n.value]
+
+
+def find_max_used_vertex(graph: Graph2DCSR) -> int:
+    """find_max_used_vertex (mpi/benchmark_helper.hpp:510-528)."""
+    return graph.info.max_used_vertex
+
+
+# ---------------------------------------------------------------------------
+# (c) BFS -- the BfsBase method set
+# ---------------------------------------------------------------------------
+class BfsOnGPU:
+    """BfsBase (mpi/bfs.hpp:29-2649) on one B200.
+
+    construct -> prepare_bfs -> run_bfs(root, pred) / get_pred -> end_bfs, as
+    mpi/main.cc drives BfsOnCPU.
+    """
+
+    def __init__(self, device: int = 0, reorder_mode: int = 2):
+        self.device = device
+        self.reorder_mode = reorder_mode
+        self.graph_: Graph2DCSR | None = None
+        self.h = None
+        self.last_stats = BfsStats()
+
+    # bfs.hpp:102-113
+    def construct(self, edge_list, keep_edges: bool = True) -> None:
+        if isinstance(edge_list, EdgeList) and edge_list.edges is None:
+            self.graph_ = Graph2DCSR.generate(edge_list.scale, edge_list.edgefactor, self.reorder_mode, self.device)
+        else:
+            edges = edge_list.edges if isinstance(edge_list, EdgeList) else edge_list
+            self.graph_ = Graph2DCSR.build(edges, self.reorder_mode, keep_edges, self.device)
+
+    # bfs.hpp:115-118
+    def prepare_bfs(self, alpha: float = 2000.0, beta: float = 8.0, count_edges: bool = False) -> None:
+        if self.graph_ is None:
+            raise G500Error(G500_E_STATE, "construct() first")
+        h = C.c_void_p()
+        check(lib().g500_bfs_create(self.graph_.h, C.byref(h)))
+        self.h = h
+        self.set_params(alpha, beta, count_edges)
+
+    def set_params(self, alpha: float = 2000.0, beta: float = 8.0, count_edges: bool = False) -> None:
+        check(lib().g500_bfs_set_params(self.h, alpha, beta, int(count_edges)))
+
+    # bfs.hpp:120, :2651-2940
+    def run_bfs(self, root: int, pred) -> BfsStats:
+        if self.h is None:
+            raise G500Error(G500_E_STATE, "prepare_bfs() first")
+        ptr, dev = _ptr(pred)
+        st = BfsStats()
+        check(lib().g500_bfs_run(self.h, int(root), ptr, int(dev), C.byref(st)))
+        self.last_stats = st
+        return st
+
+    # bfs.hpp:122-124 (no-op in the reference too: run_bfs already wrote pred)
+    def get_pred(self, pred) -> None:
+        return None
+
+    def level_stats(self) -> list[dict]:
+        arr = (LevelStats * 4096)()
+        n = C.c_int()
+        check(lib().g500_bfs_level_stats(self.h, arr, 4096, C.byref(n)))
+        keys = [f[0] for f in LevelStats._fields_]
+        return [{k: getattr(arr[i], k) for k in keys} for i in range(min(n.value, 4096))]
+
+    def device_pred_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib().g500_bfs_device_pred(self.h, C.byref(p)))
+        return p.value or 0
+
+    # bfs.hpp:126-128
+    def end_bfs(self) -> None:
+        if self.h is not None:
+            check(lib().g500_bfs_destroy(self.h))
+            self.h = None
+
+    def close(self) -> None:
+        self.end_bfs()
+        if self.graph_ is not None:
+            self.graph_.close()
+            self.graph_ = None
+
+
+# ---------------------------------------------------------------------------
+# (d) validation
+# ---------------------------------------------------------------------------
+def validate_bfs_result(graph: Graph2DCSR, root: int, pred, edge_list=None) -> tuple[bool, int, dict]:
+    """validate_bfs_result (mpi/validate.hpp:1008-1019) on the GPU.
+
+    nglobalverts = max_used_vertex + 1 and nlocalverts = pred_size, as
+    mpi/main.cc:129-133 calls it.  edge_list None uses the graph's resident
+    edge list.  Returns (ok, edge_visit_count, per-stage error counts).
+    """
+    pptr, pdev = _ptr(pred)
+    eptr, edev, m = None, 1, 0
+    if edge_list is not None:
+        edges = edge_list.edges if isinstance(edge_list, EdgeList) else edge_list
+        eptr, d = _ptr(edges)
+        edev, m = int(d), len(edges)
+    evc, ok, rep = C.c_int64(), C.c_int(), ValidateReport()
+    check(lib().g500_validate(graph.h, eptr, m, edev, int(root), pptr, int(pdev), C.byref(evc), C.byref(ok),
+                              C.byref(rep)))
+    return bool(ok.value), evc.value, {f[0]: getattr(rep, f[0]) for f in ValidateReport._fields_}
+
+
+def levels_from_pred(pred: np.ndarray) -> np.ndarray:
+    """(pred >> 48) & 0xFFFF with 0xFFFF for unreached (validate.hpp:813)."""
+    lv = ((pred >> 48) & 0xFFFF).astype(np.uint16)
+    lv[pred == -1] = 0xFFFF
+    return lv

@@ -1,0 +1,143 @@
+// Internal declarations shared by the CUDA translation units of libg500.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string>
+#include <vector>
+
+#include "../../include/g500.h"
+
+namespace g500 {
+
+// ------------------------------------------------------------------ errors
+int set_error(int code, const char* fmt, ...);
+int cuda_error(cudaError_t e, const char* what, const char* file, int line);
+
+#define G500_CUDA(call)                                                        \
+  do {                                                                         \
+    cudaError_t e__ = (call);                                                  \
+    if (e__ != cudaSuccess) return ::g500::cuda_error(e__, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define G500_TRY(call)                                                         \
+  do {                                                                         \
+    int s__ = (call);                                                          \
+    if (s__ != G500_OK) return s__;                                            \
+  } while (0)
+
+constexpr unsigned FULL_MASK = 0xFFFFFFFFu;
+constexpr int64_t LOCAL_VERTS_UNIT = 65536;  // max(11, 16) bits, bfs.hpp:109 + graph_constructor.hpp:557
+constexpr int TD_CHUNK = 256;                // edges per top-down work item
+constexpr uint32_t NO_VERTEX = 0xFFFFFFFFu;
+
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+inline int64_t roundup(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
+inline int msb_index(uint64_t v) { return 63 - __builtin_clzll(v); }
+inline int bits_for(uint64_t n) {  // smallest b with (1 << b) >= n
+  int b = 0;
+  while ((uint64_t(1) << b) < n) ++b;
+  return b;
+}
+
+int num_sms();
+
+// device allocation helpers (set the library error on failure)
+int dev_alloc(void** p, size_t bytes, const char* what);
+template <typename T>
+int dev_alloc_n(T** p, int64_t n, const char* what) {
+  return dev_alloc(reinterpret_cast<void**>(p), sizeof(T) * (size_t)(n > 0 ? n : 1), what);
+}
+void dev_free(void* p);
+
+// ------------------------------------------------------------- primitives
+// Exclusive prefix sum of n values (uint32 or uint64 input) into uint64
+// out[0..n]; out[n] = total.  tmp: scan_tmp_bytes(n) bytes of device memory.
+size_t scan_tmp_bytes(int64_t n);
+int exclusive_scan_u32(const uint32_t* in, uint64_t* out, int64_t n, void* tmp, cudaStream_t s);
+int exclusive_scan_u64(const uint64_t* in, uint64_t* out, int64_t n, void* tmp, cudaStream_t s);
+
+// Stable LSD radix sort of 64-bit keys on bits [lo_bit, hi_bit), 8 bits a
+// pass.  Sorts keys (n) using alt (n) as the ping-pong buffer; *result is the
+// buffer holding the sorted keys (keys or alt).  tmp: sort_tmp_bytes(n).
+size_t sort_tmp_bytes(int64_t n);
+int radix_sort_u64(uint64_t* keys, uint64_t* alt, int64_t n, int lo_bit, int hi_bit,
+                   void* tmp, cudaStream_t s, uint64_t** result);
+
+// -------------------------------------------------------------- generator
+struct GenPlan;  // defined in gen.cu
+int gen_edges_device(int scale, uint64_t seed1, uint64_t seed2, int64_t start, int64_t end,
+                     g500_packed_edge* out, cudaStream_t s);
+
+// 5x5 transition matrices mod 2^31-1 on the host
+struct Mat5 { uint32_t m[25]; };
+void mrg_skip_matrix_host(int byte_index, int val, Mat5* out);
+void mat5_mul_host(const Mat5& a, const Mat5& b, Mat5* r);
+void mrg_seed_host(uint64_t s1, uint64_t s2, uint32_t z[5]);
+void mrg_skip_host(uint32_t z[5], uint64_t hi, uint64_t mid, uint64_t lo);
+uint32_t mrg_next_host(uint32_t z[5]);
+void scramble_values_host(uint64_t s1, uint64_t s2, uint64_t* v0, uint64_t* v1);
+
+}  // namespace g500
+
+// --------------------------------------------------------------- handles
+struct g500_graph {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int reorder_mode = 0;
+  int log_bits = 0;                 // bits of a reordered id used in sort keys
+  int64_t log_orig_global_verts = 0;
+  int64_t nolv = 0;                 // pred_size / num_orig_local_verts
+  int64_t nlv = 0;                  // num_local_verts (multiple of 65536)
+  int64_t ngv = 0;                  // vertices with >= 1 edge
+  int64_t nge = 0;                  // directed CSR entries
+  int64_t max_used_vertex = 0;
+  int64_t device_bytes = 0;
+  double gen_seconds = 0, build_seconds = 0;
+
+  uint64_t* d_offsets = nullptr;    // [nlv + 1]
+  uint32_t* d_cols = nullptr;       // [nge]   reordered targets, ascending per row
+  uint32_t* d_first = nullptr;      // [nlv]   first (smallest) neighbour or NO_VERTEX
+  uint32_t* d_reorder = nullptr;    // [nolv]  original -> reordered
+  uint32_t* d_invert = nullptr;     // [nolv]  reordered -> original
+  uint32_t* d_vis_init = nullptr;   // [nlv/32] ~has_edge in reordered space
+  uint32_t* d_endp = nullptr;       // [nlv]   input endpoint occurrences per reordered vertex
+  g500_packed_edge* d_edges = nullptr;  // resident input edge list (optional)
+  int64_t num_edges = 0;
+  bool owns_edges = false;
+
+  std::vector<uint32_t> h_has_edge_orig;  // bitmap over original ids
+};
+
+// Device counters of one BFS level.
+struct BfsCounters {
+  unsigned long long q_items;       // top-down work items appended
+  unsigned long long discovered;    // vertices found this level
+  unsigned long long scanned;       // BU: unvisited vertices examined
+  unsigned long long edges;         // edges examined (counting mode)
+  unsigned long long sectors;       // 32-byte adjacency sectors (counting mode)
+  unsigned long long frontier;      // TD: frontier vertices
+  unsigned long long pad[2];
+};
+
+struct g500_bfs {
+  g500_graph* g = nullptr;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  double alpha = 2000.0, beta = 8.0;
+  int count_edges = 0;
+
+  int64_t* d_pred = nullptr;        // [nolv]
+  uint32_t* d_vis[2] = {nullptr, nullptr};
+  uint2* d_queue[2] = {nullptr, nullptr};
+  int64_t queue_cap = 0;
+  BfsCounters* d_counters = nullptr;   // [2]: ping-pong per level
+  BfsCounters* h_counters = nullptr;   // pinned mirror
+  unsigned long long* d_reach = nullptr;  // [2] reached vertices, nedge*2
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> level_events;  // one per level boundary
+
+  std::vector<g500_level_stats> levels;
+};

@@ -1,0 +1,184 @@
+/*
+ * g500.h -- C ABI of the B200-native Graph500 BFS hot path (libg500.so).
+ *
+ * Plain C types only: pointers, sizes, status codes.  Every function returns
+ * G500_OK (0) or a G500_E_* status; g500_last_error() gives the message of the
+ * calling thread's last failure.  No exception crosses this boundary.
+ *
+ * Each entry point replaces one step of the suzumura/graph500 reference,
+ * cited below as path:line inside that project.  Vertex ids at this boundary
+ * are the reference's ORIGINAL (scrambled, int64) ids; the reordered ids the
+ * kernels use internally never leave the library.
+ *
+ * Threading: a handle is used by one host thread at a time.  All work of a
+ * handle is ordered on that handle's CUDA stream.  Handles of different
+ * graphs are independent.
+ */
+#ifndef G500_H
+#define G500_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define G500_ABI_VERSION 1
+
+enum g500_status {
+  G500_OK = 0,
+  G500_E_INVAL = 1,    /* bad argument (null handle, out-of-range root, ...) */
+  G500_E_NOMEM = 2,    /* device or pinned-host allocation failed */
+  G500_E_DEVICE = 3,   /* a CUDA call failed (message has the CUDA error) */
+  G500_E_TIMEOUT = 4,  /* a bounded device-side wait gave up */
+  G500_E_RANGE = 5,    /* size beyond what the format or a fixed buffer holds */
+  G500_E_STATE = 6,    /* call out of order (e.g. run before create) */
+  G500_E_VALIDATION = 7
+};
+
+/* The reference's packed edge: 48-bit endpoints in 12 bytes
+ * (mpi/primitives.hpp:51-81, UnweightedPackedEdge). */
+typedef struct g500_packed_edge {
+  uint32_t v0_low;
+  uint32_t v1_low;
+  uint32_t high; /* v0[47:32] | v1[47:32] << 16 */
+} g500_packed_edge;
+
+typedef struct g500_graph g500_graph;
+typedef struct g500_bfs g500_bfs;
+typedef struct g500_msbfs g500_msbfs;
+
+/* Scalars of the built graph (mpi/graph_constructor.hpp:24-143, Graph2DCSR). */
+typedef struct g500_graph_info {
+  int64_t log_orig_global_verts; /* estimated SCALE (graph_constructor.hpp:754-759) */
+  int64_t pred_size;             /* pred[] length = num_orig_local_verts (:64) */
+  int64_t num_local_verts;       /* reordered range, multiple of 65536 (:338-346) */
+  int64_t num_global_verts;      /* vertices with >= 1 edge (:1444-1464) */
+  int64_t num_global_edges;      /* directed CSR entries after dedup (:1438-1441) */
+  int64_t max_used_vertex;       /* largest original id with an edge (benchmark_helper.hpp:510) */
+  int64_t num_input_edges;       /* length of the resident edge list (0 if not kept) */
+  int64_t device_bytes;          /* device memory held by the graph */
+  int32_t reorder_mode;          /* VERTEX_REORDERING 0/1/2 (parameters.h:37-41) */
+  int32_t device;
+} g500_graph_info;
+
+/* ------------------------------------------------------------------ misc */
+const char* g500_last_error(void);
+int g500_abi_version(void);
+/* Pinned host memory for fast host<->device copies (cudaHostAlloc). */
+int g500_host_alloc(uint64_t bytes, void** out);
+int g500_host_free(void* p);
+
+/* ------------------------------------------------------ (a) generation */
+/* The two scramble words of the generator (graph_generator.hpp:375-384). */
+int g500_scramble_values(int scale, uint64_t userseed1, uint64_t userseed2,
+                         uint64_t* val0, uint64_t* val1);
+
+/* Edges [start, end) of the spec-2010 Kronecker graph, bit-exact to
+ * RmatGraphGenerator<..,5700,1900>::generateRange (graph_generator.hpp:612-627,
+ * called from generate_graph_spec2010, benchmark_helper.hpp:308-314).
+ * out: end-start packed edges, device memory if out_on_device else host
+ * memory.  stream: a cudaStream_t or NULL for the library's own stream. */
+int g500_gen_edges(int scale, int edgefactor, uint64_t userseed1, uint64_t userseed2,
+                   int64_t start, int64_t end, g500_packed_edge* out, int out_on_device,
+                   void* stream);
+
+/* ---------------------------------------------------- (b) construction */
+/* BfsBase::construct(EdgeList*) (mpi/bfs.hpp:102-113 ->
+ * GraphConstructor2DCSR::construct, graph_constructor.hpp:554-574).
+ * edges may be host or device memory.  keep_edges != 0 keeps a device copy of
+ * the edge list for on-device validation.  reorder_mode: VERTEX_REORDERING
+ * 0 identity, 1 vertices with edges first, 2 degree descending; ties in
+ * degree are ordered by ascending original id. */
+int g500_graph_build(const g500_packed_edge* edges, int64_t num_edges, int edges_on_device,
+                     int reorder_mode, int keep_edges, int device, g500_graph** out);
+
+/* Generation + construction on the device in one call, edge list kept
+ * resident (main.cc:45-60: generate_graph_spec2010 then construct). */
+int g500_graph_generate(int scale, int edgefactor, uint64_t userseed1, uint64_t userseed2,
+                        int reorder_mode, int device, g500_graph** out);
+
+int g500_graph_info_get(const g500_graph* g, g500_graph_info* info);
+/* Graph2DCSR::has_edge (graph_constructor.hpp:101-110), original id. */
+int g500_graph_has_edge(const g500_graph* g, int64_t v, int* out);
+/* find_roots (benchmark_helper.hpp:475-508); *found = roots written. */
+int g500_graph_find_roots(const g500_graph* g, int num_roots, uint64_t userseed1,
+                          uint64_t userseed2, int64_t* roots, int* found);
+/* The resident device edge list, if kept (NULL otherwise). */
+int g500_graph_edges(const g500_graph* g, const g500_packed_edge** dev_edges, int64_t* num_edges);
+/* Host copies of the CSR for inspection: offsets[num_local_verts+1],
+ * cols[num_global_edges] (reordered ids), reorder_map[pred_size] (original ->
+ * reordered).  Any pointer may be NULL. */
+int g500_graph_copy_csr(const g500_graph* g, uint64_t* offsets, uint32_t* cols,
+                        uint32_t* reorder_map);
+/* Seconds spent on the device in generation and construction. */
+int g500_graph_timings(const g500_graph* g, double* generation_s, double* construction_s);
+int g500_graph_destroy(g500_graph* g);
+
+/* ------------------------------------------------------------ (c) BFS */
+/* Per-level record of a run (bfs.hpp:2831-2887 prints the same quantities). */
+typedef struct g500_level_stats {
+  int32_t direction;       /* 1 top-down, 0 bottom-up */
+  int32_t level;
+  int64_t frontier;        /* TD: frontier vertices */
+  int64_t discovered;      /* vertices found at this level */
+  int64_t scanned;         /* BU: unvisited vertices with edges scanned */
+  int64_t edge_sectors;    /* TD: sum ceil(deg/8); BU: sum ceil(k/8) (if counting on) */
+  int64_t edges_examined;  /* TD: sum deg; BU: sum k (if counting on) */
+  double device_ms;        /* CUDA-event time of this level's kernels */
+} g500_level_stats;
+
+typedef struct g500_bfs_stats {
+  double device_ms;        /* CUDA-event time of the whole run on the device */
+  double host_ms;          /* host wall time of the call (includes any D2H copy) */
+  int64_t reached;         /* vertices with a level */
+  int64_t nedge;           /* input edges inside the reached component */
+  int32_t num_levels;
+  int32_t td_levels;
+  int32_t bu_levels;
+  int32_t kernel_launches; /* kernels this library launched for the run */
+} g500_bfs_stats;
+
+/* BfsBase::prepare_bfs / allocate_memory (bfs.hpp:115-118, :151-239). */
+int g500_bfs_create(g500_graph* g, g500_bfs** out);
+/* alpha / beta: denominators of the direction switch (DENOM_TOPDOWN_TO_BOTTOMUP
+ * 2000, DEMON_BOTTOMUP_TO_TOPDOWN 8; parameters.h:87-88, bfs.hpp:2799-2829).
+ * count_edges != 0 records edge_sectors/edges_examined per level (slower). */
+int g500_bfs_set_params(g500_bfs* b, double alpha, double beta, int count_edges);
+/* Use this stream for the runs (NULL = the handle's own stream). */
+int g500_bfs_set_stream(g500_bfs* b, void* stream);
+/* BfsBase::run_bfs(root, pred) (bfs.hpp:120, :2651-2940): writes EVERY entry
+ * of pred[pred_size]: parent | level << 48 for reached vertices, root = root,
+ * -1 otherwise.  pred is device memory if pred_on_device else host memory
+ * (the call then returns after the device-to-host copy).  stats may be NULL. */
+int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_on_device,
+                 g500_bfs_stats* stats);
+/* Per-level records of the last run. */
+int g500_bfs_level_stats(const g500_bfs* b, g500_level_stats* out, int max_levels, int* num_levels);
+/* The device pred[] of the last run (valid until the next run or destroy). */
+int g500_bfs_device_pred(const g500_bfs* b, const int64_t** dev_pred);
+/* BfsBase::end_bfs / deallocate_memory (bfs.hpp:126-128). */
+int g500_bfs_destroy(g500_bfs* b);
+
+/* ------------------------------------------------------ (d) validation */
+typedef struct g500_validate_report {
+  int64_t range_errors;                /* validate.hpp:822-839 */
+  int64_t root_errors;                 /* :529-537, :930-933 */
+  int64_t self_parent_errors;          /* :542-571 */
+  int64_t depth_errors;                /* :920-995 */
+  int64_t edge_errors;                 /* :688-702 */
+  int64_t missing_parent_edge_errors;  /* :780-792 */
+} g500_validate_report;
+
+/* validate_bfs_result (validate.hpp:1008-1019) with nglobalverts =
+ * max_used_vertex + 1 and nlocalverts = pred_size, as main.cc:129-133 calls
+ * it.  edges == NULL uses the graph's resident edge list.  *ok = 1 when the
+ * result is valid; *edge_visit_count = the traversed-edge count TEPS uses. */
+int g500_validate(g500_graph* g, const g500_packed_edge* edges, int64_t num_edges,
+                  int edges_on_device, int64_t root, const int64_t* pred, int pred_on_device,
+                  int64_t* edge_visit_count, int* ok, g500_validate_report* report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

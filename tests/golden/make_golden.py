@@ -1,0 +1,89 @@
+"""Generate the golden fixtures of tests/golden/ from the UNMODIFIED reference.
+
+Runs the reference CPU path (suzumura/graph500, compiled here by
+oracle/Makefile against a single-rank MPI stand-in) through oracle.Reference
+and stores, per (SCALE, VERTEX_REORDERING) case:
+  - a digest of the whole generated edge list plus its first/last 64 edges,
+  - the graph scalars (graph_constructor.hpp), the find_roots roots,
+  - per root: edge_visit_count, a digest of the level array ((pred>>48)&0xFFFF),
+    the level histogram, and for two roots the full level array,
+  - one reference predecessor array (SCALE 12, VR 0, first root).
+pf_nedge.json restates the reference's known-answer table pf_nedge[]
+(mpi/utils.hpp:3663-3707, edgefactor 16, seeds 2/3).
+
+Each (SCALE, VR) case runs in its own process because the reference keeps
+global state.  Usage: python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+CASES = [(10, 0, 16), (12, 0, 16), (12, 2, 16), (16, 0, 16), (16, 2, 16), (18, 2, 8)]
+
+# mpi/utils.hpp:3663-3699: expected traversed edges for edgefactor 16, seeds (2, 3)
+PF_NEDGE = [-1, 32, 64, 128, 256, 512, 1024, 2048, 4096, 8192, 16383, 32767, 65535, 131070, 262144, 524285,
+            1048570, 2097137, 4194250, 8388513, 16776976, 33553998, 67108130, 134216177, 268432547, 536865258,
+            1073731075, 2147462776, 4294927670, 8589858508, 17179724952, 34359466407, 68718955183, 137437972330,
+            274876029861, 549752273512, 1099505021204]
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def one_case(scale: int, vr: int, nroots: int) -> None:
+    import oracle as O
+    ref = O.Reference(vr)
+    ref.generate(scale, 16)
+    edges = ref.edges()
+    ref.construct()
+    roots = ref.find_roots(nroots)
+    ref.prepare_bfs()
+    rec = {"scale": scale, "vr": vr, "info": ref.info, "roots": roots.tolist(), "num_edges": len(edges),
+           "edges_sha256": digest(edges), "per_root": []}
+    full = {}
+    for i, r in enumerate(roots):
+        pred, _ = ref.run_bfs(int(r))
+        ok, evc = ref.validate(int(r), pred)
+        assert ok, (scale, vr, r)
+        lv = ((pred >> 48) & 0xFFFF).astype(np.uint16)
+        lv[pred == -1] = 0xFFFF
+        hist = np.bincount(np.where(lv == 0xFFFF, 0, lv.astype(np.int64) + 1)).tolist()
+        rec["per_root"].append({"root": int(r), "edge_visit_count": evc, "levels_sha256": digest(lv),
+                                "level_hist": hist})
+        if i < 2:
+            full[f"levels_{i}"] = lv
+        if scale == 12 and vr == 0 and i == 0:
+            full["pred_0"] = pred
+    name = f"ref_s{scale}_vr{vr}"
+    with open(os.path.join(HERE, name + ".json"), "w") as f:
+        json.dump(rec, f, indent=1)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), edges_head=edges[:64], edges_tail=edges[-64:], **full)
+    print("wrote", name, file=sys.stderr)
+
+
+def main() -> None:
+    if len(sys.argv) == 4:
+        one_case(int(sys.argv[1]), int(sys.argv[2]), int(sys.argv[3]))
+        return
+    with open(os.path.join(HERE, "pf_nedge.json"), "w") as f:
+        json.dump({"source": "mpi/utils.hpp:3663-3707 (edgefactor 16, seeds 2/3)", "pf_nedge": PF_NEDGE}, f,
+                  indent=1)
+    env = dict(os.environ, NO_AFFINITY="1")
+    for scale, vr, nroots in CASES:
+        subprocess.run([sys.executable, __file__, str(scale), str(vr), str(nroots)], check=True, env=env,
+                       stdout=subprocess.DEVNULL)
+
+
+if __name__ == "__main__":
+    main()
