@@ -1,26 +1,31 @@
 // Direction-optimizing BFS on the device: BfsBase::run_bfs
-// (mpi/bfs.hpp:2651-2940) for one GPU.
+// (mpi/bfs.hpp:2651-2940) for one GPU, as ONE persistent cooperative kernel
+// per BFS.  Levels are separated by a grid barrier (bounded spin: on timeout
+// the kernel sets an error flag and every block returns); each block takes
+// the same direction decision from the same level counters, so no host round
+// trip happens between levels.
 //
 // State in HBM (reordered ids, nlv vertices, bitmaps of 32-bit words):
 //   vis[2]    visited bitmaps (ping-pong for bottom-up snapshots); vertices
-//             without edges start visited (bfs.hpp:262-265)
+//             without edges start visited (initialize_memory, bfs.hpp:262-265)
 //   queue[2]  top-down work items (vertex, chunk): a row is cut into chunks of
-//             TD_CHUNK edges so one hub does not serialise a warp
-//   pred      int64 per ORIGINAL id, written once per discovered vertex with
-//             parent | level << 48 (bfs.hpp:1203, :2470); -1 elsewhere
+//             TD_CHUNK edges so a hub spreads over many warps
+//   pred      int64 per ORIGINAL id: parent | level << 48 (bfs.hpp:1203,
+//             :2470), root = root (:498), -1 unreached
 //
-// Top-down (top_down_search, bfs.hpp:1139-1166, :1249-1364): each warp takes
-// 32 work items, prefix-sums their lengths and walks the concatenated edge
-// list 32 edges at a time (coalesced adjacency reads); a target whose visited
-// bit is clear is claimed with atomicOr and the winner writes pred and appends
-// the target's chunks to the next queue.
+// Top-down (top_down_search, bfs.hpp:1139-1166, :1249-1364): a warp takes B
+// work items (B adapts to the queue length so every warp has work), prefix-
+// sums their lengths and walks the concatenated edges TD_UNROLL*32 at a time;
+// a target whose visited bit is clear is claimed with atomicOr, and the
+// winner writes pred and appends the target's chunks to the next queue.
 //
-// Bottom-up (bottom_up_search_bitmap, bfs.hpp:1839-2038): each lane owns one
-// unvisited vertex of a 32-vertex word; it tests the first (smallest-id,
-// highest-degree under VERTEX_REORDERING=2) neighbour first -- the reference's
-// isolated first edge -- then scans the row until a neighbour visited before
-// this level is found.  New bits of a word are formed by one ballot, so the
-// next visited bitmap is written without atomics.
+// Bottom-up (bottom_up_search_bitmap, bfs.hpp:1839-2038): lane l owns vertex
+// l of a 32-vertex word, BU_WORDS words in flight per warp.  It tests the
+// first (smallest reordered id; under VERTEX_REORDERING=2 the highest-degree)
+// neighbour -- the reference's isolated first edge -- then scans the row until
+// a neighbour visited before this level is found; long rows are scanned by
+// the whole warp.  New bits of a word come from one ballot, so the next
+// visited bitmap is written without atomics.
 //
 // Direction switch (bfs.hpp:2799-2829): TD -> BU when growing and
 // nq > num_global_verts / alpha; BU -> TD (and stop growing) when
@@ -32,15 +37,35 @@
 
 namespace g500 {
 
-struct BfsArgs {
+constexpr int BFS_THREADS = 256;
+constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
+constexpr int BU_WORDS = 4;               // 32-vertex words a warp keeps in flight
+constexpr int BU_SERIAL = 6;              // row entries a lane checks alone before the warp helps
+constexpr unsigned long long SPIN_LIMIT = 1ull << 25;  // ~ seconds of __nanosleep(64)
+
+struct RunParams {
   const uint64_t* __restrict__ off;
   const uint32_t* __restrict__ col;
   const uint32_t* __restrict__ first;
   const uint32_t* __restrict__ invert;
+  const uint32_t* __restrict__ reorder;
+  const uint32_t* __restrict__ vis_init;
   int64_t* __restrict__ pred;
-  int64_t nlv;
-  int64_t nwords;
+  uint32_t* vis[2];
+  uint2* queue[2];
+  BfsCtl* ctl;
+  LevelRecord* rec;
+  int64_t nolv, nlv, nwords, ngv, cap;
+  int64_t root;
+  double alpha, beta;
+  int count_edges;
 };
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
   const int lane = threadIdx.x & 31;
@@ -52,67 +77,103 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
   return x;
 }
 
-__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x) {
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
 #pragma unroll
   for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(FULL_MASK, x, o);
   return x;
 }
 
-__device__ __forceinline__ uint32_t chunks_of(uint64_t deg) {
-  return (uint32_t)((deg + TD_CHUNK - 1) / TD_CHUNK);
+__device__ __forceinline__ uint32_t chunks_of(uint64_t deg) { return (uint32_t)((deg + TD_CHUNK - 1) / TD_CHUNK); }
+
+__device__ __forceinline__ void flush_counter(unsigned long long* c, unsigned long long v) {
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(c, v);
 }
 
-// Append the top-down work items of the discovered vertices of this warp.
-// nch = number of chunks of the lane's vertex (0 = nothing to expand).
-__device__ __forceinline__ void append_items(uint32_t w, uint32_t nch, uint2* __restrict__ q_out, int64_t cap,
-                                             BfsCounters* cnt, unsigned* err) {
+// Grid-wide barrier for a cooperative launch.  Thread 0 of each block arrives
+// on a counter; the last arrival bumps the generation.  Waiters spin with a
+// bound; on timeout (or an error raised elsewhere) the barrier reports failure
+// and the caller returns.  On success thread 0 also copies the counter slot
+// the next decision reads into shared memory.
+__device__ bool grid_sync(BfsCtl* ctl, const unsigned long long* slot, unsigned long long* sh_cnt,
+                          unsigned* sh_flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = &ctl->bar_gen;
+    volatile unsigned* err = &ctl->err;
+    const unsigned g = *gen;
+    __threadfence();
+    bool ok = true;
+    if (atomicAdd(&ctl->bar_count, 1u) == gridDim.x - 1) {
+      ctl->bar_count = 0;
+      __threadfence();
+      atomicAdd(&ctl->bar_gen, 1u);
+    } else {
+      unsigned long long spins = 0;
+      while (*gen == g) {
+        if (*err) { ok = false; break; }
+        if (++spins > SPIN_LIMIT) {
+          atomicOr(&ctl->err, (unsigned)BFS_ERR_TIMEOUT);
+          ok = false;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (*err) ok = false;
+    *sh_flag = ok ? 1u : 0u;
+    if (ok && slot) {
+      volatile const unsigned long long* vs = slot;
+      for (int i = 0; i < C_NUM; ++i) sh_cnt[i] = vs[i];
+    }
+  }
+  __syncthreads();
+  return *sh_flag != 0;
+}
+
+// Append the work items of the lanes' discovered vertices (nch chunks each).
+__device__ __forceinline__ void append_items(const uint32_t* w, const uint32_t* nch, uint2* __restrict__ q_out,
+                                             int64_t cap, unsigned long long* qcount, BfsCtl* ctl) {
   const int lane = threadIdx.x & 31;
-  uint32_t incl = warp_incl_scan(nch);
-  uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
+  uint32_t mine = 0;
+#pragma unroll
+  for (int j = 0; j < TD_UNROLL; ++j) mine += nch[j];
+  const uint32_t incl = warp_incl_scan(mine);
+  const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
   if (total == 0) return;
   unsigned long long base = 0;
-  if (lane == 31) base = atomicAdd(&cnt->q_items, (unsigned long long)total);
+  if (lane == 31) base = atomicAdd(qcount, (unsigned long long)total);
   base = __shfl_sync(FULL_MASK, base, 31);
   if (base + total > (unsigned long long)cap) {
-    if (lane == 0) atomicOr(err, 1u);
+    if (lane == 0) atomicOr(&ctl->err, (unsigned)BFS_ERR_QUEUE);
     return;
   }
-  uint64_t p = base + incl - nch;
-  for (uint32_t c = 0; c < nch; ++c) q_out[p + c] = make_uint2(w, c);
+  uint64_t pos = base + incl - mine;
+#pragma unroll
+  for (int j = 0; j < TD_UNROLL; ++j)
+    for (uint32_t c = 0; c < nch[j]; ++c) q_out[pos++] = make_uint2(w[j], c);
 }
 
-__global__ void __launch_bounds__(256) bfs_seed_kernel(BfsArgs a, uint32_t root_r, int64_t root_orig, uint32_t* vis,
-                                                       uint2* q, BfsCounters* cnt) {
-  uint64_t b = a.off[root_r], e = a.off[root_r + 1];
-  uint32_t nch = chunks_of(e - b);
-  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nch; c += gridDim.x * blockDim.x)
-    q[c] = make_uint2(root_r, c);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    vis[root_r >> 5] |= 1u << (root_r & 31);
-    a.pred[root_orig] = root_orig;  // first_expand, bfs.hpp:498
-    cnt->q_items = nch;
-  }
-}
-
-__global__ void __launch_bounds__(256) td_kernel(BfsArgs a, const uint2* __restrict__ q_in, int64_t qn,
-                                                 uint32_t* vis, uint2* __restrict__ q_out, int64_t cap,
-                                                 BfsCounters* cnt, unsigned* err, int level, int count_edges) {
+__device__ void td_phase(const RunParams& p, const uint2* __restrict__ q_in, int64_t qn, uint32_t* vis,
+                         uint2* __restrict__ q_out, unsigned long long* cnt, int64_t lvl) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t lvl = (int64_t)level << 48;
+  const int64_t per_warp = (qn + nwarps - 1) / nwarps;
+  const int B = per_warp >= 32 ? 32 : (per_warp < 1 ? 1 : (int)per_warp);  // items per warp batch
   unsigned long long found = 0, skipped = 0, frontier = 0, edges = 0, sectors = 0;
-  for (int64_t base = warp * 32; base < qn; base += nwarps * 32) {
+  for (int64_t base = warp * B; base < qn; base += nwarps * B) {
     const int64_t qi = base + lane;
     uint64_t b = 0;
     uint32_t len = 0, orig_u = 0;
-    if (qi < qn) {
-      uint2 it = q_in[qi];
-      uint64_t rb = a.off[it.x], re = a.off[it.x + 1];
+    if (lane < B && qi < qn) {
+      const uint2 it = q_in[qi];
+      const uint64_t rb = p.off[it.x], re = p.off[it.x + 1];
       b = rb + (uint64_t)it.y * TD_CHUNK;
       len = (uint32_t)((re - b) < (uint64_t)TD_CHUNK ? (re - b) : (uint64_t)TD_CHUNK);
-      orig_u = a.invert[it.x];
-      if (count_edges) {
+      orig_u = p.invert[it.x];
+      if (p.count_edges) {
         frontier += (it.y == 0);
         edges += len;
         sectors += (len + 7) / 8;
@@ -121,223 +182,330 @@ __global__ void __launch_bounds__(256) td_kernel(BfsArgs a, const uint2* __restr
     const uint32_t incl = warp_incl_scan(len);
     const uint32_t excl = incl - len;
     const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
-    for (uint32_t kb = 0; kb < total; kb += 32) {
-      const uint32_t k = kb + lane;
-      // owner item of virtual edge k: the last lane whose prefix is <= k
-      int o = 0;
+    for (uint32_t kb = 0; kb < total; kb += 32 * TD_UNROLL) {
+      uint32_t w[TD_UNROLL], uo[TD_UNROLL], nch[TD_UNROLL];
+      bool won[TD_UNROLL];
 #pragma unroll
-      for (int step = 16; step; step >>= 1) {
-        uint32_t ex = __shfl_sync(FULL_MASK, excl, o + step);
-        if (ex <= k) o += step;
+      for (int j = 0; j < TD_UNROLL; ++j) {
+        const uint32_t k = kb + j * 32 + lane;
+        int o = 0;  // owner item of virtual edge k: the last lane whose prefix is <= k
+#pragma unroll
+        for (int step = 16; step; step >>= 1) {
+          const uint32_t ex = __shfl_sync(FULL_MASK, excl, o + step);
+          if (ex <= k) o += step;
+        }
+        const uint64_t bo = __shfl_sync(FULL_MASK, b, o);
+        const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
+        uo[j] = __shfl_sync(FULL_MASK, orig_u, o);
+        w[j] = (k < total) ? __ldg(p.col + bo + (k - exo)) : NO_VERTEX;
       }
-      const uint64_t bo = __shfl_sync(FULL_MASK, b, o);
-      const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
-      const uint32_t uo = __shfl_sync(FULL_MASK, orig_u, o);
-      bool won = false;
-      uint32_t w = 0, nch = 0;
-      if (k < total) {
-        w = a.col[bo + (k - exo)];
-        const uint32_t bit = 1u << (w & 31);
-        uint32_t* wp = vis + (w >> 5);
-        if (!(__ldcg(wp) & bit)) won = !(atomicOr(wp, bit) & bit);
+#pragma unroll
+      for (int j = 0; j < TD_UNROLL; ++j) {
+        won[j] = false;
+        if (w[j] != NO_VERTEX) {
+          const uint32_t bit = 1u << (w[j] & 31);
+          uint32_t* wp = vis + (w[j] >> 5);
+          if (!(__ldcg(wp) & bit)) won[j] = !(atomicOr(wp, bit) & bit);
+        }
       }
-      if (won) {
-        a.pred[a.invert[w]] = (int64_t)uo | lvl;
-        uint64_t d = a.off[w + 1] - a.off[w];
-        nch = d >= 2 ? chunks_of(d) : 0;  // a degree-1 vertex only leads back to its parent
+#pragma unroll
+      for (int j = 0; j < TD_UNROLL; ++j) {
+        nch[j] = 0;
+        if (won[j]) {
+          p.pred[p.invert[w[j]]] = (int64_t)uo[j] | lvl;
+          const uint64_t d = p.off[w[j] + 1] - p.off[w[j]];
+          nch[j] = d >= 2 ? chunks_of(d) : 0;  // a degree-1 vertex only leads back to its parent
+          skipped += (d < 2);
+        }
+        found += won[j];
       }
-      found += __popc(__ballot_sync(FULL_MASK, won));
-      skipped += __popc(__ballot_sync(FULL_MASK, won && nch == 0));
-      append_items(w, nch, q_out, cap, cnt, err);
+      append_items(w, nch, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
     }
   }
-  if (lane == 0 && found) atomicAdd(&cnt->discovered, found);
-  if (lane == 0 && skipped) atomicAdd(&cnt->pad[1], skipped);
-  if (count_edges) {
-    frontier = warp_sum_u64(frontier);
-    edges = warp_sum_u64(edges);
-    sectors = warp_sum_u64(sectors);
-    if (lane == 0) {
-      atomicAdd(&cnt->frontier, frontier);
-      atomicAdd(&cnt->edges, edges);
-      atomicAdd(&cnt->sectors, sectors);
-    }
+  flush_counter(&cnt[C_DISC], found);
+  flush_counter(&cnt[C_SKIP], skipped);
+  if (p.count_edges) {
+    flush_counter(&cnt[C_FRONT], frontier);
+    flush_counter(&cnt[C_EDGES], edges);
+    flush_counter(&cnt[C_SECT], sectors);
   }
 }
 
-constexpr int BU_SERIAL = 6;  // row entries a lane checks on its own before the warp helps
+__device__ __forceinline__ bool vis_test(const uint32_t* __restrict__ vis, uint32_t v) {
+  return (__ldg(vis + (v >> 5)) >> (v & 31)) & 1u;
+}
 
-__global__ void __launch_bounds__(256) bu_kernel(BfsArgs a, const uint32_t* __restrict__ vis_cur,
-                                                 uint32_t* __restrict__ vis_next, BfsCounters* cnt, int level,
-                                                 int count_edges) {
+__device__ void bu_phase(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* __restrict__ vis_next,
+                         unsigned long long* cnt, int64_t lvl) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t lvl = (int64_t)level << 48;
   unsigned long long found = 0, scanned = 0, edges = 0, sectors = 0;
-  for (int64_t wbase = warp * 32; wbase < a.nwords; wbase += nwarps * 32) {
+  for (int64_t wbase = warp * 32; wbase < p.nwords; wbase += nwarps * 32) {
     const int64_t wi = wbase + lane;
-    const uint32_t vw = wi < a.nwords ? __ldg(vis_cur + wi) : ~0u;
-    if (wi < a.nwords && vw == ~0u) vis_next[wi] = vw;
+    const uint32_t vw = wi < p.nwords ? __ldg(vis_cur + wi) : ~0u;
+    if (wi < p.nwords && vw == ~0u) vis_next[wi] = vw;
     unsigned todo = __ballot_sync(FULL_MASK, vw != ~0u);
     while (todo) {
-      const int j = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const int64_t word = wbase + j;
-      const uint32_t wv = __shfl_sync(FULL_MASK, vw, j);
-      const int64_t v = word * 32 + lane;
-      const bool active = !((wv >> lane) & 1u);
-      uint32_t parent = NO_VERTEX;
-      uint64_t pos = 0, end = 0;
-      uint32_t k = 0;
-      const uint32_t p = active ? __ldg(a.first + v) : NO_VERTEX;
-      if (p != NO_VERTEX) {  // every unvisited vertex has an edge (vertices without one start visited)
-        k = 1;
-        if ((__ldg(vis_cur + (p >> 5)) >> (p & 31)) & 1u) {
-          parent = p;
-        } else {
-          pos = __ldg(a.off + v) + 1;
-          end = __ldg(a.off + v + 1);
-          for (int s = 0; s < BU_SERIAL && pos < end; ++s, ++pos) {
-            const uint32_t c = __ldg(a.col + pos);
-            ++k;
-            if ((__ldg(vis_cur + (c >> 5)) >> (c & 31)) & 1u) {
-              parent = c;
-              break;
-            }
+      int js[BU_WORDS];
+      uint32_t wv[BU_WORDS], parent[BU_WORDS], k[BU_WORDS];
+      uint64_t pos[BU_WORDS], end[BU_WORDS];
+#pragma unroll
+      for (int u = 0; u < BU_WORDS; ++u) {
+        js[u] = todo ? __ffs(todo) - 1 : -1;
+        todo &= todo ? todo - 1 : 0u;
+      }
+      // first neighbours of up to BU_WORDS words, all loads in flight together
+#pragma unroll
+      for (int u = 0; u < BU_WORDS; ++u) {
+        wv[u] = __shfl_sync(FULL_MASK, vw, js[u] < 0 ? 0 : js[u]);
+        if (js[u] < 0) wv[u] = ~0u;
+        const bool active = !((wv[u] >> lane) & 1u);
+        parent[u] = active ? __ldg(p.first + (wbase + js[u]) * 32 + lane) : NO_VERTEX;
+        k[u] = 0;
+        pos[u] = end[u] = 0;
+      }
+#pragma unroll
+      for (int u = 0; u < BU_WORDS; ++u) {
+        if (parent[u] != NO_VERTEX) {  // every unvisited vertex has an edge (vertices without one start visited)
+          k[u] = 1;
+          if (!vis_test(vis_cur, parent[u])) {
+            const int64_t v = (wbase + js[u]) * 32 + lane;
+            pos[u] = __ldg(p.off + v) + 1;
+            end[u] = __ldg(p.off + v + 1);
+            parent[u] = NO_VERTEX;
           }
         }
       }
-      // rows still unresolved: the whole warp scans them one at a time
-      unsigned rest = __ballot_sync(FULL_MASK, active && parent == NO_VERTEX && pos < end);
-      while (rest) {
-        const int r = __ffs(rest) - 1;
-        rest &= rest - 1;
-        const uint64_t rb = __shfl_sync(FULL_MASK, pos, r);
-        const uint64_t re = __shfl_sync(FULL_MASK, end, r);
-        uint32_t hitc = NO_VERTEX;
-        uint64_t hitpos = re;
-        for (uint64_t p0 = rb; p0 < re; p0 += 32) {
-          const uint64_t pp = p0 + lane;
-          bool h = false;
-          uint32_t c = 0;
-          if (pp < re) {
-            c = __ldg(a.col + pp);
-            h = (__ldg(vis_cur + (c >> 5)) >> (c & 31)) & 1u;
-          }
-          const unsigned hm = __ballot_sync(FULL_MASK, h);
-          if (hm) {
-            const int hl = __ffs(hm) - 1;
-            hitc = __shfl_sync(FULL_MASK, c, hl);
-            hitpos = p0 + hl;
+      // rows whose first neighbour missed: a few entries alone, then the warp
+#pragma unroll
+      for (int u = 0; u < BU_WORDS; ++u) {
+        for (int s = 0; s < BU_SERIAL && pos[u] < end[u]; ++s, ++pos[u]) {
+          const uint32_t c = __ldg(p.col + pos[u]);
+          ++k[u];
+          if (vis_test(vis_cur, c)) {
+            parent[u] = c;
+            pos[u] = end[u];
             break;
           }
         }
-        if (lane == r) {
-          parent = hitc;
-          k += (uint32_t)(min(hitpos + 1, re) - rb);
+        unsigned rest = __ballot_sync(FULL_MASK, pos[u] < end[u]);
+        while (rest) {
+          const int r = __ffs(rest) - 1;
+          rest &= rest - 1;
+          const uint64_t rb = __shfl_sync(FULL_MASK, pos[u], r);
+          const uint64_t re = __shfl_sync(FULL_MASK, end[u], r);
+          uint32_t hitc = NO_VERTEX;
+          uint64_t hitpos = re;
+          for (uint64_t p0 = rb; p0 < re; p0 += 32) {
+            const uint64_t pp = p0 + lane;
+            bool h = false;
+            uint32_t c = 0;
+            if (pp < re) {
+              c = __ldg(p.col + pp);
+              h = vis_test(vis_cur, c);
+            }
+            const unsigned hm = __ballot_sync(FULL_MASK, h);
+            if (hm) {
+              const int hl = __ffs(hm) - 1;
+              hitc = __shfl_sync(FULL_MASK, c, hl);
+              hitpos = p0 + hl;
+              break;
+            }
+          }
+          if (lane == r) {
+            parent[u] = hitc;
+            k[u] += (uint32_t)((hitpos + 1 < re ? hitpos + 1 : re) - rb);
+          }
         }
       }
-      const bool hit = parent != NO_VERTEX;
-      const unsigned hits = __ballot_sync(FULL_MASK, hit);
-      if (lane == 0) {
-        vis_next[word] = wv | hits;
-        found += __popc(hits);
-        scanned += __popc(~wv);
-      }
-      if (hit) a.pred[a.invert[v]] = (int64_t)a.invert[parent] | lvl;
-      if (count_edges) {
-        edges += k;
-        sectors += (k + 7) / 8;
+#pragma unroll
+      for (int u = 0; u < BU_WORDS; ++u) {
+        if (js[u] < 0) continue;
+        const bool hit = parent[u] != NO_VERTEX;
+        const unsigned hits = __ballot_sync(FULL_MASK, hit);
+        if (lane == 0) {
+          vis_next[wbase + js[u]] = wv[u] | hits;
+          found += __popc(hits);
+          scanned += __popc(~wv[u]);
+        }
+        if (hit) p.pred[p.invert[(wbase + js[u]) * 32 + lane]] = (int64_t)p.invert[parent[u]] | lvl;
+        if (p.count_edges) {
+          edges += k[u];
+          sectors += (k[u] + 7) / 8;
+        }
       }
     }
   }
-  found = warp_sum_u64(found);
-  scanned = warp_sum_u64(scanned);
-  if (lane == 0) {
-    if (found) atomicAdd(&cnt->discovered, found);
-    if (scanned) atomicAdd(&cnt->scanned, scanned);
-  }
-  if (count_edges) {
-    edges = warp_sum_u64(edges);
-    sectors = warp_sum_u64(sectors);
-    if (lane == 0) {
-      atomicAdd(&cnt->edges, edges);
-      atomicAdd(&cnt->sectors, sectors);
-    }
+  flush_counter(&cnt[C_DISC], found);
+  flush_counter(&cnt[C_SCAN], scanned);
+  if (p.count_edges) {
+    flush_counter(&cnt[C_EDGES], edges);
+    flush_counter(&cnt[C_SECT], sectors);
   }
 }
 
-// Bottom-up -> top-down: the vertices found by the last bottom-up level
-// (vis_new & ~vis_old) become top-down work items.
-__global__ void __launch_bounds__(256) front_to_queue_kernel(BfsArgs a, const uint32_t* __restrict__ vis_new,
-                                                             const uint32_t* __restrict__ vis_old, uint2* q_out,
-                                                             int64_t cap, BfsCounters* cnt, unsigned* err) {
+// Bottom-up -> top-down: vertices found by the last bottom-up level
+// (vis_new & ~vis_old) become work items.
+__device__ void compact_phase(const RunParams& p, const uint32_t* __restrict__ vis_new,
+                              const uint32_t* __restrict__ vis_old, uint2* q_out, unsigned long long* cnt) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long skipped = 0;
-  for (int64_t wbase = warp * 32; wbase < a.nwords; wbase += nwarps * 32) {
+  for (int64_t wbase = warp * 32; wbase < p.nwords; wbase += nwarps * 32) {
     const int64_t wi = wbase + lane;
-    const uint32_t f = wi < a.nwords ? (vis_new[wi] & ~vis_old[wi]) : 0u;
+    const uint32_t f = wi < p.nwords ? (__ldcg(vis_new + wi) & ~__ldcg(vis_old + wi)) : 0u;
     unsigned todo = __ballot_sync(FULL_MASK, f != 0);
     while (todo) {
-      const int j = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const uint32_t fj = __shfl_sync(FULL_MASK, f, j);
-      const uint32_t w = (uint32_t)((wbase + j) * 32 + lane);
-      uint32_t nch = 0;
-      const bool in = (fj >> lane) & 1u;
-      if (in) {
-        uint64_t d = a.off[w + 1] - a.off[w];
-        nch = d >= 2 ? chunks_of(d) : 0;
+      uint32_t w[TD_UNROLL], nch[TD_UNROLL];
+#pragma unroll
+      for (int j = 0; j < TD_UNROLL; ++j) {
+        w[j] = 0;
+        nch[j] = 0;
+        if (!todo) continue;
+        const int jw = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const uint32_t fj = __shfl_sync(FULL_MASK, f, jw);
+        w[j] = (uint32_t)((wbase + jw) * 32 + lane);
+        if ((fj >> lane) & 1u) {
+          const uint64_t d = p.off[w[j] + 1] - p.off[w[j]];
+          nch[j] = d >= 2 ? chunks_of(d) : 0;
+          skipped += (d < 2);
+        }
       }
-      skipped += __popc(__ballot_sync(FULL_MASK, in && nch == 0));
-      append_items(w, nch, q_out, cap, cnt, err);
+      append_items(w, nch, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
     }
   }
-  if (lane == 0 && skipped) atomicAdd(&cnt->pad[1], skipped);
+  flush_counter(&cnt[C_SKIP], skipped);
 }
 
-// reached vertices and the input edges inside the reached component
-// (sum of endpoint occurrences / 2 = validate.hpp's edge_visit_count for a valid tree)
-__global__ void __launch_bounds__(256) reach_kernel(const uint32_t* __restrict__ vis,
+__global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(RunParams p) {
+  __shared__ unsigned long long sh_cnt[C_NUM];
+  __shared__ unsigned sh_flag;
+  BfsCtl* ctl = p.ctl;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+
+  // initialize_memory (bfs.hpp:241-276): pred = -1, visited = ~has_edge
+  if (tid == 0) ctl->t0_ns = globaltimer();
+  for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = -1;
+  for (int64_t i = tid; i < p.nwords; i += nthreads) p.vis[0][i] = p.vis_init[i];
+  if (blockIdx.x == 0 && threadIdx.x < 3 * C_NUM) (&ctl->cnt[0][0])[threadIdx.x] = 0;
+  const uint32_t root_r = p.reorder[p.root];
+  const bool has_edges = (int64_t)root_r < p.nlv && p.first[root_r] != NO_VERTEX;
+  uint64_t root_deg = has_edges ? p.off[root_r + 1] - p.off[root_r] : 0;
+  const int64_t root_items = (int64_t)chunks_of(root_deg);
+  if (!grid_sync(ctl, nullptr, sh_cnt, &sh_flag)) return;
+
+  // first_expand (bfs.hpp:477-518)
+  for (int64_t c = tid; c < root_items; c += nthreads) p.queue[0][c] = make_uint2(root_r, (uint32_t)c);
+  if (tid == 0) {
+    p.pred[p.root] = p.root;
+    if (has_edges) p.vis[0][root_r >> 5] |= 1u << (root_r & 31);
+    ctl->root_has_edges = has_edges ? 1 : 0;
+  }
+  if (!has_edges) {
+    if (tid == 0) {
+      ctl->num_levels = 0;
+      ctl->final_vis = 0;
+      ctl->t_end_ns = globaltimer();
+    }
+    return;
+  }
+  if (!grid_sync(ctl, nullptr, sh_cnt, &sh_flag)) return;
+  if (tid == 0) ctl->t_init_ns = globaltimer();
+
+  int cur_vis = 0, cur_q = 0;
+  bool forward = true, growing = true;
+  int64_t qn = root_items, prev_nq = 0, visited = 1, carried = 0;
+  unsigned phase = 0;
+  int level = 1;
+  for (;; ++level) {
+    unsigned long long* cnt = ctl->cnt[phase % 3];
+    if (blockIdx.x == 0 && threadIdx.x < C_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
+    const int64_t lvl = (int64_t)level << 48;
+    if (forward) td_phase(p, p.queue[cur_q], qn, p.vis[cur_vis], p.queue[cur_q ^ 1], cnt, lvl);
+    else bu_phase(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], cnt, lvl);
+    if (!grid_sync(ctl, cnt, sh_cnt, &sh_flag)) return;
+    ++phase;
+    const int64_t nq = (int64_t)sh_cnt[C_DISC];
+    if (tid == 0) {
+      LevelRecord r;
+      r.direction = forward ? 1 : 0;
+      r.level = level;
+      r.frontier = forward ? sh_cnt[C_FRONT] + carried : 0;
+      r.discovered = nq;
+      r.scanned = sh_cnt[C_SCAN];
+      r.edges = sh_cnt[C_EDGES] + (forward ? carried : 0);
+      r.sectors = sh_cnt[C_SECT] + (forward ? carried : 0);
+      r.t_ns = globaltimer();
+      p.rec[level - 1] = r;
+    }
+    visited += nq;
+    const bool was_forward = forward;
+    if (!forward) cur_vis ^= 1;  // the bottom-up output is the current visited map
+    if (nq == 0) break;
+    if (level >= MAX_LEVELS) {
+      if (tid == 0) atomicOr(&ctl->err, (unsigned)BFS_ERR_DEPTH);
+      break;
+    }
+    const int64_t unvisited = p.ngv - visited;
+    if (growing && nq > prev_nq) {
+      if (forward && (double)nq > (double)p.ngv / p.alpha) forward = false;
+    } else if (!forward && unvisited < (int64_t)((double)p.ngv / p.beta)) {
+      forward = true;
+      growing = false;
+    }
+    prev_nq = nq;
+    if (forward) {
+      if (was_forward) {
+        cur_q ^= 1;
+        qn = (int64_t)sh_cnt[C_QITEMS];
+        carried = (int64_t)sh_cnt[C_SKIP];
+      } else {
+        unsigned long long* ccnt = ctl->cnt[phase % 3];
+        if (blockIdx.x == 0 && threadIdx.x < C_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
+        compact_phase(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], p.queue[cur_q], ccnt);
+        if (!grid_sync(ctl, ccnt, sh_cnt, &sh_flag)) return;
+        ++phase;
+        qn = (int64_t)sh_cnt[C_QITEMS];
+        carried = (int64_t)sh_cnt[C_SKIP];
+      }
+      if (qn > p.cap) {  // append_items already flagged it; never read past the queue
+        if (tid == 0) atomicOr(&ctl->err, (unsigned)BFS_ERR_QUEUE);
+        return;
+      }
+    }
+  }
+  if (tid == 0) {
+    ctl->num_levels = (unsigned)level;
+    ctl->final_vis = cur_vis;
+    ctl->t_end_ns = globaltimer();
+  }
+}
+
+// reached vertices and 2 x the input edges inside the reached component
+// (sum of endpoint occurrences = 2 x validate.hpp's edge_visit_count for a valid tree)
+__global__ void __launch_bounds__(256) reach_kernel(const uint32_t* vis0, const uint32_t* vis1,
                                                     const uint32_t* __restrict__ vis_init,
                                                     const uint32_t* __restrict__ endp, int64_t nwords,
-                                                    unsigned long long* out) {
+                                                    BfsCtl* ctl) {
+  if (!ctl->root_has_edges) return;
+  const uint32_t* vis = ctl->final_vis ? vis1 : vis0;
   unsigned long long reached = 0, e2 = 0;
   for (int64_t wi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; wi < nwords;
        wi += (int64_t)gridDim.x * blockDim.x) {
     uint32_t bits = vis[wi] & ~vis_init[wi];
     reached += __popc(bits);
     while (bits) {
-      int b = __ffs(bits) - 1;
+      const int b = __ffs(bits) - 1;
       bits &= bits - 1;
       e2 += endp[wi * 32 + b];
     }
   }
-  reached = warp_sum_u64(reached);
-  e2 = warp_sum_u64(e2);
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&out[0], reached);
-    atomicAdd(&out[1], e2);
-  }
-}
-
-static int level_event(g500_bfs* b, size_t i) {
-  while (b->level_events.size() <= i) {
-    cudaEvent_t e;
-    G500_CUDA(cudaEventCreate(&e));
-    b->level_events.push_back(e);
-  }
-  return G500_OK;
-}
-
-static unsigned persistent_grid(const void* kernel, int threads) {
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
-  if (per_sm <= 0) per_sm = 1;
-  return (unsigned)(num_sms() * per_sm);
+  flush_counter(&ctl->reach[0], reached);
+  flush_counter(&ctl->reach[1], e2);
 }
 
 }  // namespace g500
@@ -353,12 +521,11 @@ static int bfs_free(g500_bfs* b) {
   dev_free(b->d_vis[1]);
   dev_free(b->d_queue[0]);
   dev_free(b->d_queue[1]);
-  dev_free(b->d_counters);
-  dev_free(b->d_reach);
-  if (b->h_counters) cudaFreeHost(b->h_counters);
+  dev_free(b->d_ctl);
+  dev_free(b->d_rec);
+  if (b->h_ctl) cudaFreeHost(b->h_ctl);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
-  for (cudaEvent_t e : b->level_events) cudaEventDestroy(e);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
   delete b;
   return G500_OK;
@@ -382,11 +549,23 @@ extern "C" int g500_bfs_create(g500_graph* g, g500_bfs** out) {
   if (st == G500_OK) st = dev_alloc_n(&b->d_vis[1], nwords, "visited bitmap");
   if (st == G500_OK) st = dev_alloc_n(&b->d_queue[0], b->queue_cap, "top-down queue");
   if (st == G500_OK) st = dev_alloc_n(&b->d_queue[1], b->queue_cap, "top-down queue");
-  if (st == G500_OK) st = dev_alloc_n(&b->d_counters, 2, "level counters");
-  if (st == G500_OK) st = dev_alloc_n(&b->d_reach, 4, "reach counters");
-  if (st == G500_OK) chk(cudaHostAlloc(&b->h_counters, 2 * sizeof(BfsCounters), cudaHostAllocDefault), "cudaHostAlloc");
+  if (st == G500_OK) st = dev_alloc_n(&b->d_ctl, 1, "bfs control block");
+  if (st == G500_OK) st = dev_alloc_n(&b->d_rec, MAX_LEVELS, "level records");
+  if (st == G500_OK) chk(cudaHostAlloc(&b->h_ctl, sizeof(BfsCtl), cudaHostAllocDefault), "cudaHostAlloc");
+  if (st == G500_OK) chk(cudaMemset(b->d_ctl, 0, sizeof(BfsCtl)), "cudaMemset");
+  if (st == G500_OK) memset(b->h_ctl, 0, sizeof(BfsCtl));
   chk(cudaEventCreate(&b->ev0), "cudaEventCreate");
   chk(cudaEventCreate(&b->ev1), "cudaEventCreate");
+  if (st == G500_OK) {
+    int per_sm = 0;
+    chk(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_persistent_kernel, BFS_THREADS, 0),
+        "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    int coop = 0;
+    chk(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, g->device), "cudaDeviceGetAttribute");
+    if (st == G500_OK && (!coop || per_sm <= 0))
+      st = set_error(G500_E_DEVICE, "device cannot co-schedule the persistent BFS kernel");
+    b->grid = (unsigned)(num_sms() * std::max(per_sm, 1));
+  }
   if (st != G500_OK) {
     bfs_free(b);
     return st;
@@ -413,160 +592,105 @@ extern "C" int g500_bfs_set_stream(g500_bfs* b, void* stream) {
 extern "C" int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_on_device, g500_bfs_stats* stats) {
   if (!b) return set_error(G500_E_INVAL, "null bfs");
   g500_graph* g = b->g;
-  if (root < 0 || root >= g->nolv) return set_error(G500_E_INVAL, "root %lld outside [0, %lld)", (long long)root,
-                                                    (long long)g->nolv);
+  if (root < 0 || root >= g->nolv)
+    return set_error(G500_E_INVAL, "root %lld outside [0, %lld)", (long long)root, (long long)g->nolv);
   if (!pred) return set_error(G500_E_INVAL, "null pred");
   G500_CUDA(cudaSetDevice(g->device));
   auto t0 = std::chrono::steady_clock::now();
   cudaStream_t s = b->stream;
-  int64_t* d_pred = pred_on_device ? pred : b->d_pred;
-  const int64_t nwords = g->nlv / 32;
-  uint32_t root_r = 0;
-  G500_CUDA(cudaMemcpyAsync(&root_r, g->d_reorder + root, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  G500_CUDA(cudaStreamSynchronize(s));
-  BfsArgs a{g->d_offsets, g->d_cols, g->d_first, g->d_invert, d_pred, g->nlv, nwords};
-  const bool root_has_edges = (int64_t)root_r < g->nlv && ((g->h_has_edge_orig[(size_t)(root >> 5)] >> (root & 31)) & 1u);
-  const unsigned grid_td = persistent_grid((const void*)td_kernel, 256);
-  const unsigned grid_bu = persistent_grid((const void*)bu_kernel, 256);
-  int launches = 0;
-  b->levels.clear();
-
+  RunParams p;
+  p.off = g->d_offsets;
+  p.col = g->d_cols;
+  p.first = g->d_first;
+  p.invert = g->d_invert;
+  p.reorder = g->d_reorder;
+  p.vis_init = g->d_vis_init;
+  p.pred = pred_on_device ? pred : b->d_pred;
+  p.vis[0] = b->d_vis[0];
+  p.vis[1] = b->d_vis[1];
+  p.queue[0] = b->d_queue[0];
+  p.queue[1] = b->d_queue[1];
+  p.ctl = b->d_ctl;
+  p.rec = b->d_rec;
+  p.nolv = g->nolv;
+  p.nlv = g->nlv;
+  p.nwords = g->nlv / 32;
+  p.ngv = g->ngv;
+  p.cap = b->queue_cap;
+  p.root = root;
+  p.alpha = b->alpha;
+  p.beta = b->beta;
+  p.count_edges = b->count_edges;
+  void* args[] = {&p};
+  G500_CUDA(cudaMemsetAsync(b->d_ctl, 0, sizeof(BfsCtl), s));
   G500_CUDA(cudaEventRecord(b->ev0, s));
-  // initialize_memory (bfs.hpp:241-276): pred = -1, visited = ~has_edge
-  G500_CUDA(cudaMemsetAsync(d_pred, 0xFF, sizeof(int64_t) * g->nolv, s));
-  int64_t root_val = root;
-  if (!root_has_edges) {
-    G500_CUDA(cudaMemcpyAsync(d_pred + root, &root_val, sizeof(int64_t), cudaMemcpyHostToDevice, s));
-  } else {
-    G500_CUDA(cudaMemcpyAsync(b->d_vis[0], g->d_vis_init, sizeof(uint32_t) * nwords, cudaMemcpyDeviceToDevice, s));
-    G500_CUDA(cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(BfsCounters), s));
-    bfs_seed_kernel<<<4, 256, 0, s>>>(a, root_r, root, b->d_vis[0], b->d_queue[0], b->d_counters);
+  G500_CUDA(cudaLaunchCooperativeKernel((const void*)bfs_persistent_kernel, dim3(b->grid), dim3(BFS_THREADS), args,
+                                        0, s));
+  G500_CUDA(cudaEventRecord(b->ev1, s));
+  if (stats) {
+    const unsigned rg = (unsigned)std::min<int64_t>(ceil_div(std::max<int64_t>(p.nwords, 1), 256), num_sms() * 8);
+    reach_kernel<<<rg, 256, 0, s>>>(b->d_vis[0], b->d_vis[1], g->d_vis_init, g->d_endp, p.nwords, b->d_ctl);
     G500_CUDA(cudaGetLastError());
-    ++launches;
-    G500_CUDA(cudaMemcpyAsync(b->h_counters, b->d_counters, sizeof(BfsCounters), cudaMemcpyDeviceToHost, s));
-    G500_CUDA(cudaStreamSynchronize(s));
-    int64_t qn = (int64_t)b->h_counters[0].q_items;
-    int cur_vis = 0, cur_q = 0;
-    bool forward = true, growing = true;
-    int64_t prev_nq = 0, visited = 1;
-    int64_t carried = 0;  // degree-1 frontier vertices the queue skips: 1 edge, 1 sector each
-    unsigned* d_err = reinterpret_cast<unsigned*>(&b->d_counters[1].pad[0]);
-    for (int level = 1;; ++level) {
-      if (level > 0xFFFE) return set_error(G500_E_RANGE, "BFS depth exceeds the 16-bit level field");
-      G500_TRY(level_event(b, 2 * (level - 1)));
-      G500_CUDA(cudaEventRecord(b->level_events[2 * (level - 1)], s));
-      G500_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(BfsCounters), s));
-      g500_level_stats ls;
-      memset(&ls, 0, sizeof(ls));
-      ls.level = level;
-      ls.direction = forward ? 1 : 0;
-      if (forward) {
-        if (qn > 0) {
-          td_kernel<<<grid_td, 256, 0, s>>>(a, b->d_queue[cur_q], qn, b->d_vis[cur_vis], b->d_queue[cur_q ^ 1],
-                                            b->queue_cap, b->d_counters, d_err, level, b->count_edges);
-          G500_CUDA(cudaGetLastError());
-          ++launches;
-        }
-      } else {
-        bu_kernel<<<grid_bu, 256, 0, s>>>(a, b->d_vis[cur_vis], b->d_vis[cur_vis ^ 1], b->d_counters, level,
-                                          b->count_edges);
-        G500_CUDA(cudaGetLastError());
-        ++launches;
-      }
-      G500_TRY(level_event(b, 2 * (level - 1) + 1));
-      G500_CUDA(cudaEventRecord(b->level_events[2 * (level - 1) + 1], s));
-      G500_CUDA(cudaMemcpyAsync(b->h_counters, b->d_counters, 2 * sizeof(BfsCounters), cudaMemcpyDeviceToHost, s));
-      G500_CUDA(cudaStreamSynchronize(s));
-      const BfsCounters c = b->h_counters[0];
-      float lms = 0;
-      G500_CUDA(cudaEventElapsedTime(&lms, b->level_events[2 * (level - 1)], b->level_events[2 * (level - 1) + 1]));
-      ls.device_ms = lms;
-      if (b->h_counters[1].pad[0]) return set_error(G500_E_RANGE, "top-down queue overflow");
-      const int64_t nq = (int64_t)c.discovered;
-      ls.discovered = nq;
-      ls.frontier = forward ? (int64_t)c.frontier + carried : 0;
-      ls.scanned = (int64_t)c.scanned;
-      ls.edges_examined = (int64_t)c.edges + (forward ? carried : 0);
-      ls.edge_sectors = (int64_t)c.sectors + (forward ? carried : 0);
-      carried = (int64_t)c.pad[1];
-      b->levels.push_back(ls);
-      visited += nq;
-      const bool was_forward = forward;
-      if (!forward) cur_vis ^= 1;  // the BU output becomes the current visited map
-      if (nq == 0) break;
-      const int64_t unvisited = g->ngv - visited;
-      if (growing && nq > prev_nq) {
-        if (forward && (double)nq > (double)g->ngv / b->alpha) forward = false;
-      } else {
-        if (!forward && unvisited < (int64_t)((double)g->ngv / b->beta)) {
-          forward = true;
-          growing = false;
-        }
-      }
-      prev_nq = nq;
-      if (forward) {
-        if (was_forward) {
-          cur_q ^= 1;
-          qn = (int64_t)c.q_items;
-        } else {
-          // BU -> TD: the last BU level's discoveries become work items
-          G500_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(BfsCounters), s));
-          front_to_queue_kernel<<<grid_td, 256, 0, s>>>(a, b->d_vis[cur_vis], b->d_vis[cur_vis ^ 1],
-                                                        b->d_queue[cur_q], b->queue_cap, b->d_counters, d_err);
-          G500_CUDA(cudaGetLastError());
-          ++launches;
-          G500_CUDA(cudaMemcpyAsync(b->h_counters, b->d_counters, 2 * sizeof(BfsCounters), cudaMemcpyDeviceToHost, s));
-          G500_CUDA(cudaStreamSynchronize(s));
-          if (b->h_counters[1].pad[0]) return set_error(G500_E_RANGE, "top-down queue overflow");
-          qn = (int64_t)b->h_counters[0].q_items;
-          carried = (int64_t)b->h_counters[0].pad[1];
-        }
-      }
-    }
-    // the current visited map for the reach statistics
-    if (stats) {
-      G500_CUDA(cudaEventRecord(b->ev1, s));
-      G500_CUDA(cudaMemsetAsync(b->d_reach, 0, 4 * sizeof(unsigned long long), s));
-      reach_kernel<<<grid_bu, 256, 0, s>>>(b->d_vis[cur_vis], g->d_vis_init, g->d_endp, nwords, b->d_reach);
-      G500_CUDA(cudaGetLastError());
-    }
   }
-  if (!stats || !root_has_edges) G500_CUDA(cudaEventRecord(b->ev1, s));
-  if (!pred_on_device) {
-    G500_CUDA(cudaMemcpyAsync(pred, d_pred, sizeof(int64_t) * g->nolv, cudaMemcpyDeviceToHost, s));
-  }
-  unsigned long long reach[2] = {1, 0};
-  if (stats && root_has_edges)
-    G500_CUDA(cudaMemcpyAsync(reach, b->d_reach, sizeof(reach), cudaMemcpyDeviceToHost, s));
+  if (!pred_on_device)
+    G500_CUDA(cudaMemcpyAsync(pred, b->d_pred, sizeof(int64_t) * g->nolv, cudaMemcpyDeviceToHost, s));
+  G500_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s));
   G500_CUDA(cudaStreamSynchronize(s));
+  b->last_root = root;
+  const BfsCtl& c = *b->h_ctl;
+  if (c.err & BFS_ERR_TIMEOUT) return set_error(G500_E_TIMEOUT, "grid barrier wait gave up (bounded spin)");
+  if (c.err & BFS_ERR_QUEUE) return set_error(G500_E_RANGE, "top-down queue overflow");
+  if (c.err & BFS_ERR_DEPTH) return set_error(G500_E_RANGE, "BFS depth exceeds the 16-bit level field");
   if (stats) {
     float ms = 0;
     G500_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
     memset(stats, 0, sizeof(*stats));
     stats->device_ms = ms;
     stats->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    if (root_has_edges) {
-      stats->reached = (int64_t)reach[0];
-      stats->nedge = (int64_t)(reach[1] / 2);
+    if (c.root_has_edges) {
+      stats->reached = (int64_t)c.reach[0];
+      stats->nedge = (int64_t)(c.reach[1] / 2);
     } else {
-      uint32_t e = 0;
+      uint32_t root_r = 0, e = 0;
+      G500_CUDA(cudaMemcpy(&root_r, g->d_reorder + root, sizeof(uint32_t), cudaMemcpyDeviceToHost));
       G500_CUDA(cudaMemcpy(&e, g->d_endp + root_r, sizeof(uint32_t), cudaMemcpyDeviceToHost));
       stats->reached = 1;
       stats->nedge = e / 2;
     }
-    stats->num_levels = (int32_t)b->levels.size();
-    for (const auto& l : b->levels) (l.direction ? stats->td_levels : stats->bu_levels)++;
-    stats->kernel_launches = launches;
+    stats->num_levels = (int32_t)c.num_levels;
+    stats->kernel_launches = 1;
+    if (c.num_levels) {
+      std::vector<LevelRecord> rec(c.num_levels);
+      G500_CUDA(cudaMemcpy(rec.data(), b->d_rec, sizeof(LevelRecord) * c.num_levels, cudaMemcpyDeviceToHost));
+      for (const auto& r : rec) (r.direction ? stats->td_levels : stats->bu_levels)++;
+    }
   }
   return G500_OK;
 }
 
 extern "C" int g500_bfs_level_stats(const g500_bfs* b, g500_level_stats* out, int max_levels, int* n) {
   if (!b) return set_error(G500_E_INVAL, "null bfs");
-  int k = (int)std::min<size_t>(b->levels.size(), (size_t)std::max(max_levels, 0));
-  if (out)
-    for (int i = 0; i < k; ++i) out[i] = b->levels[(size_t)i];
-  if (n) *n = (int)b->levels.size();
+  const int total = (int)b->h_ctl->num_levels;
+  if (n) *n = total;
+  const int k = std::min(total, std::max(max_levels, 0));
+  if (!out || k == 0) return G500_OK;
+  G500_CUDA(cudaSetDevice(b->g->device));
+  std::vector<LevelRecord> rec((size_t)k);
+  G500_CUDA(cudaMemcpy(rec.data(), b->d_rec, sizeof(LevelRecord) * k, cudaMemcpyDeviceToHost));
+  unsigned long long prev = b->h_ctl->t_init_ns;
+  for (int i = 0; i < k; ++i) {
+    const LevelRecord& r = rec[(size_t)i];
+    g500_level_stats& o = out[i];
+    o.direction = r.direction;
+    o.level = r.level;
+    o.frontier = (int64_t)r.frontier;
+    o.discovered = (int64_t)r.discovered;
+    o.scanned = (int64_t)r.scanned;
+    o.edges_examined = (int64_t)r.edges;
+    o.edge_sectors = (int64_t)r.sectors;
+    o.device_ms = (double)(r.t_ns - prev) * 1e-6;  // %globaltimer between level barriers
+    prev = r.t_ns;
+  }
   return G500_OK;
 }
 

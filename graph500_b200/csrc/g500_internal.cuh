@@ -30,7 +30,7 @@ int cuda_error(cudaError_t e, const char* what, const char* file, int line);
 
 constexpr unsigned FULL_MASK = 0xFFFFFFFFu;
 constexpr int64_t LOCAL_VERTS_UNIT = 65536;  // max(11, 16) bits, bfs.hpp:109 + graph_constructor.hpp:557
-constexpr int TD_CHUNK = 256;                // edges per top-down work item
+constexpr int TD_CHUNK = 128;                // edges per top-down work item (one warp pass)
 constexpr uint32_t NO_VERTEX = 0xFFFFFFFFu;
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
@@ -111,16 +111,34 @@ struct g500_graph {
   std::vector<uint32_t> h_has_edge_orig;  // bitmap over original ids
 };
 
-// Device counters of one BFS level.
-struct BfsCounters {
-  unsigned long long q_items;       // top-down work items appended
-  unsigned long long discovered;    // vertices found this level
-  unsigned long long scanned;       // BU: unvisited vertices examined
-  unsigned long long edges;         // edges examined (counting mode)
-  unsigned long long sectors;       // 32-byte adjacency sectors (counting mode)
-  unsigned long long frontier;      // TD: frontier vertices
-  unsigned long long pad[2];
+// Per-phase counters of the persistent BFS kernel (3 rotating slots).
+enum BfsCounter { C_QITEMS = 0, C_DISC, C_SCAN, C_EDGES, C_SECT, C_FRONT, C_SKIP, C_NUM = 8 };
+enum BfsErr { BFS_ERR_QUEUE = 1, BFS_ERR_TIMEOUT = 2, BFS_ERR_DEPTH = 4 };
+
+// Control block of one run, in device memory.
+struct BfsCtl {
+  unsigned long long cnt[3][C_NUM];
+  unsigned bar_count;
+  unsigned bar_gen;
+  unsigned err;
+  unsigned num_levels;
+  int final_vis;
+  int root_has_edges;
+  unsigned long long t0_ns;
+  unsigned long long t_init_ns;  // pred/visited initialised and root seeded
+  unsigned long long t_end_ns;
+  unsigned long long reach[2];  // reached vertices, 2 * nedge (filled by reach_kernel)
 };
+
+// One record per level, written by the kernel.
+struct LevelRecord {
+  int32_t direction;
+  int32_t level;
+  unsigned long long frontier, discovered, scanned, edges, sectors;
+  unsigned long long t_ns;  // %globaltimer when the level's barrier completed
+};
+
+constexpr int MAX_LEVELS = 0xFFFE;
 
 struct g500_bfs {
   g500_graph* g = nullptr;
@@ -128,16 +146,15 @@ struct g500_bfs {
   cudaStream_t stream = nullptr;
   double alpha = 2000.0, beta = 8.0;
   int count_edges = 0;
+  unsigned grid = 0;                 // co-resident blocks of the persistent kernel
 
-  int64_t* d_pred = nullptr;        // [nolv]
+  int64_t* d_pred = nullptr;         // [nolv]
   uint32_t* d_vis[2] = {nullptr, nullptr};
   uint2* d_queue[2] = {nullptr, nullptr};
   int64_t queue_cap = 0;
-  BfsCounters* d_counters = nullptr;   // [2]: ping-pong per level
-  BfsCounters* h_counters = nullptr;   // pinned mirror
-  unsigned long long* d_reach = nullptr;  // [2] reached vertices, nedge*2
+  BfsCtl* d_ctl = nullptr;
+  BfsCtl* h_ctl = nullptr;           // pinned copy after each run
+  LevelRecord* d_rec = nullptr;      // [MAX_LEVELS]
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  std::vector<cudaEvent_t> level_events;  // one per level boundary
-
-  std::vector<g500_level_stats> levels;
+  int64_t last_root = -1;
 };
