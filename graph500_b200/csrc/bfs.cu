@@ -39,7 +39,7 @@ namespace g500 {
 
 constexpr int BFS_THREADS = 256;
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
-constexpr int BU_WORDS = 4;               // 32-vertex words a warp keeps in flight
+constexpr int BU_WORDS = 6;               // 32-vertex words a warp keeps in flight (pass A)
 constexpr int BU_SERIAL = 6;              // row entries a lane checks alone before the warp helps
 constexpr unsigned long long SPIN_LIMIT = 1ull << 25;  // ~ seconds of __nanosleep(64)
 
@@ -52,7 +52,7 @@ struct RunParams {
   const uint32_t* __restrict__ vis_init;
   int64_t* __restrict__ pred;
   uint32_t* vis[2];
-  uint2* queue[2];
+  TdItem* queue[2];
   BfsCtl* ctl;
   LevelRecord* rec;
   int64_t nolv, nlv, nwords, ngv, cap;
@@ -60,6 +60,8 @@ struct RunParams {
   double alpha, beta;
   int count_edges;
 };
+
+constexpr uint32_t FIRST_CHUNK = 0x80000000u;
 
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
@@ -83,11 +85,29 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
   return x;
 }
 
+// last lane whose exclusive prefix is <= k (prefixes are non-decreasing over lanes)
+__device__ __forceinline__ int owner_lane(uint32_t excl, uint32_t k) {
+  int o = 0;
+#pragma unroll
+  for (int step = 16; step; step >>= 1) {
+    const uint32_t ex = __shfl_sync(FULL_MASK, excl, o + step);
+    if (ex <= k) o += step;
+  }
+  return o;
+}
+
 __device__ __forceinline__ uint32_t chunks_of(uint64_t deg) { return (uint32_t)((deg + TD_CHUNK - 1) / TD_CHUNK); }
 
 __device__ __forceinline__ void flush_counter(unsigned long long* c, unsigned long long v) {
   v = warp_sum(v);
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(c, v);
+}
+
+// next dynamically scheduled batch index of this warp
+__device__ __forceinline__ unsigned long long grab(unsigned long long* work) {
+  unsigned long long b = 0;
+  if ((threadIdx.x & 31) == 0) b = atomicAdd(work, 1ull);
+  return __shfl_sync(FULL_MASK, b, 0);
 }
 
 // Grid-wide barrier for a cooperative launch.  Thread 0 of each block arrives
@@ -132,16 +152,18 @@ __device__ bool grid_sync(BfsCtl* ctl, const unsigned long long* slot, unsigned 
   return *sh_flag != 0;
 }
 
-// Append the work items of the lanes' discovered vertices (nch chunks each).
-__device__ __forceinline__ void append_items(const uint32_t* w, const uint32_t* nch, uint2* __restrict__ q_out,
-                                             int64_t cap, unsigned long long* qcount, BfsCtl* ctl) {
+// Append the chunks of one row per lane (deg = re - rb; rows of degree < 2 and
+// lanes with no row pass deg 0).  The whole warp writes the items, so a hub's
+// thousands of chunks are not left to one lane.
+__device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t orig, bool whole_row,
+                                           TdItem* __restrict__ q_out, int64_t cap, unsigned long long* qcount,
+                                           BfsCtl* ctl) {
   const int lane = threadIdx.x & 31;
-  uint32_t mine = 0;
-#pragma unroll
-  for (int j = 0; j < TD_UNROLL; ++j) mine += nch[j];
-  const uint32_t incl = warp_incl_scan(mine);
+  const uint32_t nch = chunks_of(deg);
+  const uint32_t incl = warp_incl_scan(nch);
   const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
   if (total == 0) return;
+  const uint32_t excl = incl - nch;
   unsigned long long base = 0;
   if (lane == 31) base = atomicAdd(qcount, (unsigned long long)total);
   base = __shfl_sync(FULL_MASK, base, 31);
@@ -149,32 +171,47 @@ __device__ __forceinline__ void append_items(const uint32_t* w, const uint32_t* 
     if (lane == 0) atomicOr(&ctl->err, (unsigned)BFS_ERR_QUEUE);
     return;
   }
-  uint64_t pos = base + incl - mine;
-#pragma unroll
-  for (int j = 0; j < TD_UNROLL; ++j)
-    for (uint32_t c = 0; c < nch[j]; ++c) q_out[pos++] = make_uint2(w[j], c);
+  for (uint32_t i0 = 0; i0 < total; i0 += 32) {
+    const uint32_t i = i0 + lane;
+    const int o = owner_lane(excl, i);
+    const uint64_t rbo = __shfl_sync(FULL_MASK, rb, o);
+    const uint64_t dego = __shfl_sync(FULL_MASK, deg, o);
+    const uint32_t origo = __shfl_sync(FULL_MASK, orig, o);
+    const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
+    (void)whole_row;
+    if (i < total) {
+      const uint64_t c = i - exo;
+      const uint64_t b = rbo + c * TD_CHUNK;
+      const uint64_t left = rbo + dego - b;
+      TdItem it;
+      it.begin = b;
+      it.orig = origo;
+      it.len = (uint32_t)(left < (uint64_t)TD_CHUNK ? left : (uint64_t)TD_CHUNK) | (c == 0 ? FIRST_CHUNK : 0u);
+      q_out[base + i] = it;
+    }
+  }
 }
 
-__device__ void td_phase(const RunParams& p, const uint2* __restrict__ q_in, int64_t qn, uint32_t* vis,
-                         uint2* __restrict__ q_out, unsigned long long* cnt, int64_t lvl) {
+__device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, int64_t qn, uint32_t* vis,
+                         TdItem* __restrict__ q_out, unsigned long long* cnt, int64_t lvl) {
   const int lane = threadIdx.x & 31;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t per_warp = (qn + nwarps - 1) / nwarps;
-  const int B = per_warp >= 32 ? 32 : (per_warp < 1 ? 1 : (int)per_warp);  // items per warp batch
+  const int B = per_warp >= 32 ? 32 : (per_warp < 1 ? 1 : (int)per_warp);  // items per batch
   unsigned long long found = 0, skipped = 0, frontier = 0, edges = 0, sectors = 0;
-  for (int64_t base = warp * B; base < qn; base += nwarps * B) {
+  for (;;) {
+    const int64_t base = (int64_t)grab(&cnt[C_WORK]) * B;
+    if (base >= qn) break;
     const int64_t qi = base + lane;
     uint64_t b = 0;
     uint32_t len = 0, orig_u = 0;
     if (lane < B && qi < qn) {
-      const uint2 it = q_in[qi];
-      const uint64_t rb = p.off[it.x], re = p.off[it.x + 1];
-      b = rb + (uint64_t)it.y * TD_CHUNK;
-      len = (uint32_t)((re - b) < (uint64_t)TD_CHUNK ? (re - b) : (uint64_t)TD_CHUNK);
-      orig_u = p.invert[it.x];
+      const TdItem it = q_in[qi];
+      b = it.begin;
+      len = it.len & ~FIRST_CHUNK;
+      orig_u = it.orig;
       if (p.count_edges) {
-        frontier += (it.y == 0);
+        frontier += (it.len >> 31);
         edges += len;
         sectors += (len + 7) / 8;
       }
@@ -183,17 +220,12 @@ __device__ void td_phase(const RunParams& p, const uint2* __restrict__ q_in, int
     const uint32_t excl = incl - len;
     const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
     for (uint32_t kb = 0; kb < total; kb += 32 * TD_UNROLL) {
-      uint32_t w[TD_UNROLL], uo[TD_UNROLL], nch[TD_UNROLL];
+      uint32_t w[TD_UNROLL], uo[TD_UNROLL];
       bool won[TD_UNROLL];
 #pragma unroll
       for (int j = 0; j < TD_UNROLL; ++j) {
         const uint32_t k = kb + j * 32 + lane;
-        int o = 0;  // owner item of virtual edge k: the last lane whose prefix is <= k
-#pragma unroll
-        for (int step = 16; step; step >>= 1) {
-          const uint32_t ex = __shfl_sync(FULL_MASK, excl, o + step);
-          if (ex <= k) o += step;
-        }
+        const int o = owner_lane(excl, k);
         const uint64_t bo = __shfl_sync(FULL_MASK, b, o);
         const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
         uo[j] = __shfl_sync(FULL_MASK, orig_u, o);
@@ -210,16 +242,19 @@ __device__ void td_phase(const RunParams& p, const uint2* __restrict__ q_in, int
       }
 #pragma unroll
       for (int j = 0; j < TD_UNROLL; ++j) {
-        nch[j] = 0;
+        uint64_t rb = 0, deg = 0;
+        uint32_t ow = 0;
         if (won[j]) {
-          p.pred[p.invert[w[j]]] = (int64_t)uo[j] | lvl;
-          const uint64_t d = p.off[w[j] + 1] - p.off[w[j]];
-          nch[j] = d >= 2 ? chunks_of(d) : 0;  // a degree-1 vertex only leads back to its parent
-          skipped += (d < 2);
+          ow = __ldg(p.invert + w[j]);
+          rb = __ldg(p.off + w[j]);
+          deg = __ldg(p.off + w[j] + 1) - rb;
+          p.pred[ow] = (int64_t)uo[j] | lvl;
+          skipped += (deg < 2);
+          if (deg < 2) deg = 0;  // a degree-1 vertex only leads back to its parent
+          ++found;
         }
-        found += won[j];
+        append_row(rb, deg, ow, true, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
       }
-      append_items(w, nch, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
     }
   }
   flush_counter(&cnt[C_DISC], found);
@@ -235,110 +270,136 @@ __device__ __forceinline__ bool vis_test(const uint32_t* __restrict__ vis, uint3
   return (__ldg(vis + (v >> 5)) >> (v & 31)) & 1u;
 }
 
-__device__ void bu_phase(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* __restrict__ vis_next,
-                         unsigned long long* cnt, int64_t lvl) {
+// Bottom-up pass A: every unvisited vertex tests its first neighbour; the
+// misses go to a list for pass B.  BU_WORDS words per warp are in flight.
+__device__ void bu_pass_a(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* __restrict__ vis_next,
+                          uint32_t* __restrict__ miss, unsigned long long* cnt, int64_t lvl) {
   const int lane = threadIdx.x & 31;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long found = 0, scanned = 0, edges = 0, sectors = 0;
-  for (int64_t wbase = warp * 32; wbase < p.nwords; wbase += nwarps * 32) {
+  unsigned long long found = 0, scanned = 0;
+  for (;;) {
+    const int64_t wbase = (int64_t)grab(&cnt[C_WORK]) * 32;
+    if (wbase >= p.nwords) break;
     const int64_t wi = wbase + lane;
     const uint32_t vw = wi < p.nwords ? __ldg(vis_cur + wi) : ~0u;
     if (wi < p.nwords && vw == ~0u) vis_next[wi] = vw;
     unsigned todo = __ballot_sync(FULL_MASK, vw != ~0u);
     while (todo) {
       int js[BU_WORDS];
-      uint32_t wv[BU_WORDS], parent[BU_WORDS], k[BU_WORDS];
-      uint64_t pos[BU_WORDS], end[BU_WORDS];
+      uint32_t wv[BU_WORDS], par[BU_WORDS];
 #pragma unroll
       for (int u = 0; u < BU_WORDS; ++u) {
         js[u] = todo ? __ffs(todo) - 1 : -1;
         todo &= todo ? todo - 1 : 0u;
-      }
-      // first neighbours of up to BU_WORDS words, all loads in flight together
-#pragma unroll
-      for (int u = 0; u < BU_WORDS; ++u) {
         wv[u] = __shfl_sync(FULL_MASK, vw, js[u] < 0 ? 0 : js[u]);
         if (js[u] < 0) wv[u] = ~0u;
-        const bool active = !((wv[u] >> lane) & 1u);
-        parent[u] = active ? __ldg(p.first + (wbase + js[u]) * 32 + lane) : NO_VERTEX;
-        k[u] = 0;
-        pos[u] = end[u] = 0;
+        par[u] = ((wv[u] >> lane) & 1u) ? NO_VERTEX : __ldg(p.first + (wbase + js[u]) * 32 + lane);
       }
+      uint32_t nmiss = 0;
+      unsigned missbits = 0;
 #pragma unroll
       for (int u = 0; u < BU_WORDS; ++u) {
-        if (parent[u] != NO_VERTEX) {  // every unvisited vertex has an edge (vertices without one start visited)
-          k[u] = 1;
-          if (!vis_test(vis_cur, parent[u])) {
-            const int64_t v = (wbase + js[u]) * 32 + lane;
-            pos[u] = __ldg(p.off + v) + 1;
-            end[u] = __ldg(p.off + v + 1);
-            parent[u] = NO_VERTEX;
-          }
+        const bool active = !((wv[u] >> lane) & 1u);  // every unvisited vertex has an edge
+        const bool hit = active && par[u] != NO_VERTEX && vis_test(vis_cur, par[u]);
+        if (active && !hit) {
+          missbits |= 1u << u;
+          ++nmiss;
         }
-      }
-      // rows whose first neighbour missed: a few entries alone, then the warp
-#pragma unroll
-      for (int u = 0; u < BU_WORDS; ++u) {
-        for (int s = 0; s < BU_SERIAL && pos[u] < end[u]; ++s, ++pos[u]) {
-          const uint32_t c = __ldg(p.col + pos[u]);
-          ++k[u];
-          if (vis_test(vis_cur, c)) {
-            parent[u] = c;
-            pos[u] = end[u];
-            break;
-          }
-        }
-        unsigned rest = __ballot_sync(FULL_MASK, pos[u] < end[u]);
-        while (rest) {
-          const int r = __ffs(rest) - 1;
-          rest &= rest - 1;
-          const uint64_t rb = __shfl_sync(FULL_MASK, pos[u], r);
-          const uint64_t re = __shfl_sync(FULL_MASK, end[u], r);
-          uint32_t hitc = NO_VERTEX;
-          uint64_t hitpos = re;
-          for (uint64_t p0 = rb; p0 < re; p0 += 32) {
-            const uint64_t pp = p0 + lane;
-            bool h = false;
-            uint32_t c = 0;
-            if (pp < re) {
-              c = __ldg(p.col + pp);
-              h = vis_test(vis_cur, c);
-            }
-            const unsigned hm = __ballot_sync(FULL_MASK, h);
-            if (hm) {
-              const int hl = __ffs(hm) - 1;
-              hitc = __shfl_sync(FULL_MASK, c, hl);
-              hitpos = p0 + hl;
-              break;
-            }
-          }
-          if (lane == r) {
-            parent[u] = hitc;
-            k[u] += (uint32_t)((hitpos + 1 < re ? hitpos + 1 : re) - rb);
-          }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < BU_WORDS; ++u) {
-        if (js[u] < 0) continue;
-        const bool hit = parent[u] != NO_VERTEX;
         const unsigned hits = __ballot_sync(FULL_MASK, hit);
-        if (lane == 0) {
+        if (js[u] >= 0 && lane == 0) {
           vis_next[wbase + js[u]] = wv[u] | hits;
           found += __popc(hits);
           scanned += __popc(~wv[u]);
         }
-        if (hit) p.pred[p.invert[(wbase + js[u]) * 32 + lane]] = (int64_t)p.invert[parent[u]] | lvl;
-        if (p.count_edges) {
-          edges += k[u];
-          sectors += (k[u] + 7) / 8;
-        }
+        if (hit) p.pred[__ldg(p.invert + (wbase + js[u]) * 32 + lane)] = (int64_t)__ldg(p.invert + par[u]) | lvl;
+      }
+      // misses -> list
+      const uint32_t incl = warp_incl_scan(nmiss);
+      const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
+      if (total) {
+        unsigned long long base = 0;
+        if (lane == 31) base = atomicAdd(&cnt[C_QITEMS], (unsigned long long)total);
+        base = __shfl_sync(FULL_MASK, base, 31) + incl - nmiss;
+#pragma unroll
+        for (int u = 0; u < BU_WORDS; ++u)
+          if (missbits & (1u << u)) miss[base++] = (uint32_t)((wbase + js[u]) * 32 + lane);
       }
     }
   }
   flush_counter(&cnt[C_DISC], found);
   flush_counter(&cnt[C_SCAN], scanned);
+  if (p.count_edges) {  // hits examined exactly one edge (one sector)
+    flush_counter(&cnt[C_EDGES], found);
+    flush_counter(&cnt[C_SECT], found);
+  }
+}
+
+// Bottom-up pass B: the rows whose first neighbour missed.  A lane checks
+// BU_SERIAL more entries alone; longer rows are scanned by the whole warp.
+__device__ void bu_pass_b(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* vis_next,
+                          const uint32_t* __restrict__ miss, int64_t nmiss, unsigned long long* cnt, int64_t lvl) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long found = 0, edges = 0, sectors = 0;
+  for (;;) {
+    const int64_t base = (int64_t)grab(&cnt[C_WORK]) * 32;
+    if (base >= nmiss) break;
+    const int64_t i = base + lane;
+    uint32_t v = NO_VERTEX, parent = NO_VERTEX, k = 0;
+    uint64_t pos = 0, end = 0;
+    if (i < nmiss) {
+      v = __ldcg(miss + i);
+      pos = __ldg(p.off + v) + 1;
+      end = __ldg(p.off + v + 1);
+      k = 1;
+      for (int s = 0; s < BU_SERIAL && pos < end; ++s, ++pos) {
+        const uint32_t c = __ldg(p.col + pos);
+        ++k;
+        if (vis_test(vis_cur, c)) {
+          parent = c;
+          pos = end;
+          break;
+        }
+      }
+    }
+    unsigned rest = __ballot_sync(FULL_MASK, pos < end);
+    while (rest) {
+      const int r = __ffs(rest) - 1;
+      rest &= rest - 1;
+      const uint64_t rb = __shfl_sync(FULL_MASK, pos, r);
+      const uint64_t re = __shfl_sync(FULL_MASK, end, r);
+      uint32_t hitc = NO_VERTEX;
+      uint64_t hitpos = re;
+      for (uint64_t p0 = rb; p0 < re; p0 += 32) {
+        const uint64_t pp = p0 + lane;
+        bool h = false;
+        uint32_t c = 0;
+        if (pp < re) {
+          c = __ldg(p.col + pp);
+          h = vis_test(vis_cur, c);
+        }
+        const unsigned hm = __ballot_sync(FULL_MASK, h);
+        if (hm) {
+          const int hl = __ffs(hm) - 1;
+          hitc = __shfl_sync(FULL_MASK, c, hl);
+          hitpos = p0 + hl;
+          break;
+        }
+      }
+      if (lane == r) {
+        parent = hitc;
+        k += (uint32_t)((hitpos + 1 < re ? hitpos + 1 : re) - rb);
+      }
+    }
+    if (parent != NO_VERTEX) {
+      atomicOr(vis_next + (v >> 5), 1u << (v & 31));
+      p.pred[__ldg(p.invert + v)] = (int64_t)__ldg(p.invert + parent) | lvl;
+      ++found;
+    }
+    if (p.count_edges && v != NO_VERTEX) {
+      edges += k;
+      sectors += (k + 7) / 8;
+    }
+  }
+  flush_counter(&cnt[C_DISC], found);
   if (p.count_edges) {
     flush_counter(&cnt[C_EDGES], edges);
     flush_counter(&cnt[C_SECT], sectors);
@@ -348,33 +409,30 @@ __device__ void bu_phase(const RunParams& p, const uint32_t* __restrict__ vis_cu
 // Bottom-up -> top-down: vertices found by the last bottom-up level
 // (vis_new & ~vis_old) become work items.
 __device__ void compact_phase(const RunParams& p, const uint32_t* __restrict__ vis_new,
-                              const uint32_t* __restrict__ vis_old, uint2* q_out, unsigned long long* cnt) {
+                              const uint32_t* __restrict__ vis_old, TdItem* q_out, unsigned long long* cnt) {
   const int lane = threadIdx.x & 31;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long skipped = 0;
-  for (int64_t wbase = warp * 32; wbase < p.nwords; wbase += nwarps * 32) {
+  for (;;) {
+    const int64_t wbase = (int64_t)grab(&cnt[C_WORK]) * 32;
+    if (wbase >= p.nwords) break;
     const int64_t wi = wbase + lane;
     const uint32_t f = wi < p.nwords ? (__ldcg(vis_new + wi) & ~__ldcg(vis_old + wi)) : 0u;
     unsigned todo = __ballot_sync(FULL_MASK, f != 0);
     while (todo) {
-      uint32_t w[TD_UNROLL], nch[TD_UNROLL];
-#pragma unroll
-      for (int j = 0; j < TD_UNROLL; ++j) {
-        w[j] = 0;
-        nch[j] = 0;
-        if (!todo) continue;
-        const int jw = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const uint32_t fj = __shfl_sync(FULL_MASK, f, jw);
-        w[j] = (uint32_t)((wbase + jw) * 32 + lane);
-        if ((fj >> lane) & 1u) {
-          const uint64_t d = p.off[w[j] + 1] - p.off[w[j]];
-          nch[j] = d >= 2 ? chunks_of(d) : 0;
-          skipped += (d < 2);
-        }
+      const int jw = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint32_t fj = __shfl_sync(FULL_MASK, f, jw);
+      const uint32_t w = (uint32_t)((wbase + jw) * 32 + lane);
+      uint64_t rb = 0, deg = 0;
+      uint32_t ow = 0;
+      if ((fj >> lane) & 1u) {
+        rb = __ldg(p.off + w);
+        deg = __ldg(p.off + w + 1) - rb;
+        ow = __ldg(p.invert + w);
+        skipped += (deg < 2);
+        if (deg < 2) deg = 0;
       }
-      append_items(w, nch, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
+      append_row(rb, deg, ow, true, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
     }
   }
   flush_counter(&cnt[C_SKIP], skipped);
@@ -394,12 +452,20 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(RunParam
   if (blockIdx.x == 0 && threadIdx.x < 3 * C_NUM) (&ctl->cnt[0][0])[threadIdx.x] = 0;
   const uint32_t root_r = p.reorder[p.root];
   const bool has_edges = (int64_t)root_r < p.nlv && p.first[root_r] != NO_VERTEX;
-  uint64_t root_deg = has_edges ? p.off[root_r + 1] - p.off[root_r] : 0;
+  const uint64_t root_b = has_edges ? p.off[root_r] : 0;
+  const uint64_t root_deg = has_edges ? p.off[root_r + 1] - root_b : 0;
   const int64_t root_items = (int64_t)chunks_of(root_deg);
   if (!grid_sync(ctl, nullptr, sh_cnt, &sh_flag)) return;
 
-  // first_expand (bfs.hpp:477-518)
-  for (int64_t c = tid; c < root_items; c += nthreads) p.queue[0][c] = make_uint2(root_r, (uint32_t)c);
+  // first_expand (bfs.hpp:477-518): the root's row becomes the first queue
+  for (int64_t c = tid; c < root_items; c += nthreads) {
+    TdItem it;
+    it.begin = root_b + (uint64_t)c * TD_CHUNK;
+    it.orig = (uint32_t)p.root;
+    const uint64_t left = root_deg - (uint64_t)c * TD_CHUNK;
+    it.len = (uint32_t)(left < (uint64_t)TD_CHUNK ? left : (uint64_t)TD_CHUNK) | (c == 0 ? FIRST_CHUNK : 0u);
+    p.queue[0][c] = it;
+  }
   if (tid == 0) {
     p.pred[p.root] = p.root;
     if (has_edges) p.vis[0][root_r >> 5] |= 1u << (root_r & 31);
@@ -409,7 +475,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(RunParam
     if (tid == 0) {
       ctl->num_levels = 0;
       ctl->final_vis = 0;
-      ctl->t_end_ns = globaltimer();
+      ctl->t_init_ns = ctl->t_end_ns = globaltimer();
     }
     return;
   }
@@ -425,20 +491,48 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(RunParam
     unsigned long long* cnt = ctl->cnt[phase % 3];
     if (blockIdx.x == 0 && threadIdx.x < C_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
     const int64_t lvl = (int64_t)level << 48;
-    if (forward) td_phase(p, p.queue[cur_q], qn, p.vis[cur_vis], p.queue[cur_q ^ 1], cnt, lvl);
-    else bu_phase(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], cnt, lvl);
-    if (!grid_sync(ctl, cnt, sh_cnt, &sh_flag)) return;
-    ++phase;
-    const int64_t nq = (int64_t)sh_cnt[C_DISC];
+    unsigned long long disc = 0, scan = 0, edges = 0, sect = 0, front = 0, skip = 0, qitems = 0;
+    if (forward) {
+      td_phase(p, p.queue[cur_q], qn, p.vis[cur_vis], p.queue[cur_q ^ 1], cnt, lvl);
+      if (!grid_sync(ctl, cnt, sh_cnt, &sh_flag)) return;
+      ++phase;
+      disc = sh_cnt[C_DISC];
+      edges = sh_cnt[C_EDGES];
+      sect = sh_cnt[C_SECT];
+      front = sh_cnt[C_FRONT];
+      skip = sh_cnt[C_SKIP];
+      qitems = sh_cnt[C_QITEMS];
+    } else {
+      uint32_t* miss = reinterpret_cast<uint32_t*>(p.queue[0]);
+      bu_pass_a(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, cnt, lvl);
+      if (!grid_sync(ctl, cnt, sh_cnt, &sh_flag)) return;
+      ++phase;
+      disc = sh_cnt[C_DISC];
+      scan = sh_cnt[C_SCAN];
+      edges = sh_cnt[C_EDGES];
+      sect = sh_cnt[C_SECT];
+      const int64_t nmiss = (int64_t)sh_cnt[C_QITEMS];
+      if (nmiss > 0) {
+        unsigned long long* cnt_b = ctl->cnt[phase % 3];
+        if (blockIdx.x == 0 && threadIdx.x < C_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
+        bu_pass_b(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, nmiss, cnt_b, lvl);
+        if (!grid_sync(ctl, cnt_b, sh_cnt, &sh_flag)) return;
+        ++phase;
+        disc += sh_cnt[C_DISC];
+        edges += sh_cnt[C_EDGES];
+        sect += sh_cnt[C_SECT];
+      }
+    }
+    const int64_t nq = (int64_t)disc;
     if (tid == 0) {
       LevelRecord r;
       r.direction = forward ? 1 : 0;
       r.level = level;
-      r.frontier = forward ? sh_cnt[C_FRONT] + carried : 0;
-      r.discovered = nq;
-      r.scanned = sh_cnt[C_SCAN];
-      r.edges = sh_cnt[C_EDGES] + (forward ? carried : 0);
-      r.sectors = sh_cnt[C_SECT] + (forward ? carried : 0);
+      r.frontier = forward ? front + carried : 0;
+      r.discovered = disc;
+      r.scanned = scan;
+      r.edges = edges + (forward ? carried : 0);
+      r.sectors = sect + (forward ? carried : 0);
       r.t_ns = globaltimer();
       p.rec[level - 1] = r;
     }
@@ -461,8 +555,8 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(RunParam
     if (forward) {
       if (was_forward) {
         cur_q ^= 1;
-        qn = (int64_t)sh_cnt[C_QITEMS];
-        carried = (int64_t)sh_cnt[C_SKIP];
+        qn = (int64_t)qitems;
+        carried = (int64_t)skip;
       } else {
         unsigned long long* ccnt = ctl->cnt[phase % 3];
         if (blockIdx.x == 0 && threadIdx.x < C_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
@@ -472,7 +566,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(RunParam
         qn = (int64_t)sh_cnt[C_QITEMS];
         carried = (int64_t)sh_cnt[C_SKIP];
       }
-      if (qn > p.cap) {  // append_items already flagged it; never read past the queue
+      if (qn > p.cap) {  // append_row already flagged it; never read past the queue
         if (tid == 0) atomicOr(&ctl->err, (unsigned)BFS_ERR_QUEUE);
         return;
       }
@@ -547,7 +641,7 @@ extern "C" int g500_bfs_create(g500_graph* g, g500_bfs** out) {
   if (st == G500_OK) st = dev_alloc_n(&b->d_pred, g->nolv, "pred");
   if (st == G500_OK) st = dev_alloc_n(&b->d_vis[0], nwords, "visited bitmap");
   if (st == G500_OK) st = dev_alloc_n(&b->d_vis[1], nwords, "visited bitmap");
-  if (st == G500_OK) st = dev_alloc_n(&b->d_queue[0], b->queue_cap, "top-down queue");
+  if (st == G500_OK) st = dev_alloc_n(&b->d_queue[0], b->queue_cap, "top-down queue / bottom-up miss list");
   if (st == G500_OK) st = dev_alloc_n(&b->d_queue[1], b->queue_cap, "top-down queue");
   if (st == G500_OK) st = dev_alloc_n(&b->d_ctl, 1, "bfs control block");
   if (st == G500_OK) st = dev_alloc_n(&b->d_rec, MAX_LEVELS, "level records");

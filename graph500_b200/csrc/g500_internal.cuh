@@ -112,7 +112,14 @@ struct g500_graph {
 };
 
 // Per-phase counters of the persistent BFS kernel (3 rotating slots).
-enum BfsCounter { C_QITEMS = 0, C_DISC, C_SCAN, C_EDGES, C_SECT, C_FRONT, C_SKIP, C_NUM = 8 };
+enum BfsCounter { C_QITEMS = 0, C_DISC, C_SCAN, C_EDGES, C_SECT, C_FRONT, C_SKIP, C_WORK, C_NUM };
+
+// Top-down work item: one chunk (<= TD_CHUNK edges) of a frontier row.
+struct __align__(16) TdItem {
+  unsigned long long begin;  // first adjacency index of the chunk
+  uint32_t orig;             // original id of the row's vertex (the parent written to pred)
+  uint32_t len;              // chunk length; bit 31 marks the row's first chunk
+};
 enum BfsErr { BFS_ERR_QUEUE = 1, BFS_ERR_TIMEOUT = 2, BFS_ERR_DEPTH = 4 };
 
 // Control block of one run, in device memory.
@@ -150,7 +157,7 @@ struct g500_bfs {
 
   int64_t* d_pred = nullptr;         // [nolv]
   uint32_t* d_vis[2] = {nullptr, nullptr};
-  uint2* d_queue[2] = {nullptr, nullptr};
+  TdItem* d_queue[2] = {nullptr, nullptr};
   int64_t queue_cap = 0;
   BfsCtl* d_ctl = nullptr;
   BfsCtl* h_ctl = nullptr;           // pinned copy after each run
