@@ -38,8 +38,9 @@
 namespace g500 {
 
 constexpr int BFS_THREADS = 256;
+constexpr int BFS_MIN_BLOCKS = 3;        // co-resident blocks per SM (80 registers, no spills)
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
-constexpr int BU_WORDS = 6;               // 32-vertex words a warp keeps in flight (pass A)
+constexpr int BU_WORDS = 4;               // 32-vertex words a warp keeps in flight
 constexpr int BU_SERIAL = 6;              // row entries a lane checks alone before the warp helps
 constexpr unsigned long long SPIN_LIMIT = 1ull << 25;  // ~ seconds of __nanosleep(64)
 
@@ -110,13 +111,28 @@ __device__ __forceinline__ unsigned long long grab(unsigned long long* work) {
   return __shfl_sync(FULL_MASK, b, 0);
 }
 
-// Grid-wide barrier for a cooperative launch.  Thread 0 of each block arrives
-// on a counter; the last arrival bumps the generation.  Waiters spin with a
-// bound; on timeout (or an error raised elsewhere) the barrier reports failure
-// and the caller returns.  On success thread 0 also copies the counter slot
-// the next decision reads into shared memory.
-__device__ bool grid_sync(BfsCtl* ctl, const unsigned long long* slot, unsigned long long* sh_cnt,
-                          unsigned* sh_flag) {
+// Add a warp's value to the block accumulator of counter i (flushed to the
+// level's global slot once per block at the next grid barrier).
+__device__ __forceinline__ void block_add(unsigned long long* sh_acc, int i, unsigned long long v) {
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh_acc[i], v);
+}
+
+// Grid-wide barrier for a cooperative launch.  The block's accumulated
+// counters are first added to flush_slot (one global atomic per counter per
+// block).  Thread 0 then arrives on a counter; the last arrival bumps the
+// generation.  Waiters spin with a bound; on timeout (or an error raised
+// elsewhere) the barrier reports failure and the caller returns.  On success
+// thread 0 copies read_slot into sh_cnt for the block's next decision.
+__device__ bool grid_sync(BfsCtl* ctl, unsigned long long* flush_slot, unsigned long long* sh_acc,
+                          const unsigned long long* read_slot, unsigned long long* sh_cnt, unsigned* sh_flag) {
+  __syncthreads();
+  if (threadIdx.x < C_NUM) {
+    const unsigned long long v = sh_acc[threadIdx.x];
+    if (flush_slot && v) atomicAdd(&flush_slot[threadIdx.x], v);
+    sh_acc[threadIdx.x] = 0;
+    __threadfence();
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* gen = &ctl->bar_gen;
@@ -143,8 +159,8 @@ __device__ bool grid_sync(BfsCtl* ctl, const unsigned long long* slot, unsigned 
     __threadfence();
     if (*err) ok = false;
     *sh_flag = ok ? 1u : 0u;
-    if (ok && slot) {
-      volatile const unsigned long long* vs = slot;
+    if (ok && read_slot) {
+      volatile const unsigned long long* vs = read_slot;
       for (int i = 0; i < C_NUM; ++i) sh_cnt[i] = vs[i];
     }
   }
@@ -152,12 +168,11 @@ __device__ bool grid_sync(BfsCtl* ctl, const unsigned long long* slot, unsigned 
   return *sh_flag != 0;
 }
 
-// Append the chunks of one row per lane (deg = re - rb; rows of degree < 2 and
-// lanes with no row pass deg 0).  The whole warp writes the items, so a hub's
-// thousands of chunks are not left to one lane.
-__device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t orig, bool whole_row,
-                                           TdItem* __restrict__ q_out, int64_t cap, unsigned long long* qcount,
-                                           BfsCtl* ctl) {
+// Append the chunks of one row per lane (rows of degree < 2 and lanes with no
+// row pass deg 0).  The whole warp writes the items, so a hub's thousands of
+// chunks are not left to one lane.
+__device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t orig, TdItem* __restrict__ q_out,
+                                           int64_t cap, unsigned long long* qcount, BfsCtl* ctl) {
   const int lane = threadIdx.x & 31;
   const uint32_t nch = chunks_of(deg);
   const uint32_t incl = warp_incl_scan(nch);
@@ -178,7 +193,6 @@ __device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t o
     const uint64_t dego = __shfl_sync(FULL_MASK, deg, o);
     const uint32_t origo = __shfl_sync(FULL_MASK, orig, o);
     const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
-    (void)whole_row;
     if (i < total) {
       const uint64_t c = i - exo;
       const uint64_t b = rbo + c * TD_CHUNK;
@@ -192,13 +206,17 @@ __device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t o
   }
 }
 
+// Top-down level: expand the work items, claim unvisited targets, and list the
+// discovered (vertex, original id) pairs.  Rows are cut into work items only
+// if the next level is top-down as well (chunk_phase).
 __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, int64_t qn, uint32_t* vis,
-                         TdItem* __restrict__ q_out, unsigned long long* cnt, int64_t lvl) {
+                         uint2* __restrict__ found_list, unsigned long long* cnt, unsigned long long* sh_acc,
+                         int64_t lvl) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t per_warp = (qn + nwarps - 1) / nwarps;
   const int B = per_warp >= 32 ? 32 : (per_warp < 1 ? 1 : (int)per_warp);  // items per batch
-  unsigned long long found = 0, skipped = 0, frontier = 0, edges = 0, sectors = 0;
+  unsigned long long found = 0, frontier = 0, edges = 0, sectors = 0;
   for (;;) {
     const int64_t base = (int64_t)grab(&cnt[C_WORK]) * B;
     if (base >= qn) break;
@@ -220,7 +238,7 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
     const uint32_t excl = incl - len;
     const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
     for (uint32_t kb = 0; kb < total; kb += 32 * TD_UNROLL) {
-      uint32_t w[TD_UNROLL], uo[TD_UNROLL];
+      uint32_t w[TD_UNROLL], uo[TD_UNROLL], ow[TD_UNROLL];
       bool won[TD_UNROLL];
 #pragma unroll
       for (int j = 0; j < TD_UNROLL; ++j) {
@@ -231,6 +249,7 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
         uo[j] = __shfl_sync(FULL_MASK, orig_u, o);
         w[j] = (k < total) ? __ldg(p.col + bo + (k - exo)) : NO_VERTEX;
       }
+      uint32_t nwon = 0;
 #pragma unroll
       for (int j = 0; j < TD_UNROLL; ++j) {
         won[j] = false;
@@ -239,43 +258,72 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
           uint32_t* wp = vis + (w[j] >> 5);
           if (!(__ldcg(wp) & bit)) won[j] = !(atomicOr(wp, bit) & bit);
         }
+        nwon += won[j];
       }
 #pragma unroll
       for (int j = 0; j < TD_UNROLL; ++j) {
-        uint64_t rb = 0, deg = 0;
-        uint32_t ow = 0;
+        ow[j] = 0;
         if (won[j]) {
-          ow = __ldg(p.invert + w[j]);
-          rb = __ldg(p.off + w[j]);
-          deg = __ldg(p.off + w[j] + 1) - rb;
-          p.pred[ow] = (int64_t)uo[j] | lvl;
-          skipped += (deg < 2);
-          if (deg < 2) deg = 0;  // a degree-1 vertex only leads back to its parent
-          ++found;
+          ow[j] = __ldg(p.invert + w[j]);
+          p.pred[ow[j]] = (int64_t)uo[j] | lvl;
         }
-        append_row(rb, deg, ow, true, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
       }
+      const uint32_t wincl = warp_incl_scan(nwon);
+      const uint32_t wtotal = __shfl_sync(FULL_MASK, wincl, 31);
+      if (wtotal) {
+        unsigned long long fb = 0;
+        if (lane == 31) fb = atomicAdd(&cnt[C_QITEMS], (unsigned long long)wtotal);
+        fb = __shfl_sync(FULL_MASK, fb, 31) + wincl - nwon;
+#pragma unroll
+        for (int j = 0; j < TD_UNROLL; ++j)
+          if (won[j]) found_list[fb++] = make_uint2(w[j], ow[j]);
+      }
+      found += nwon;
     }
   }
-  flush_counter(&cnt[C_DISC], found);
-  flush_counter(&cnt[C_SKIP], skipped);
+  block_add(sh_acc, C_DISC, found);
   if (p.count_edges) {
-    flush_counter(&cnt[C_FRONT], frontier);
-    flush_counter(&cnt[C_EDGES], edges);
-    flush_counter(&cnt[C_SECT], sectors);
+    block_add(sh_acc, C_FRONT, frontier);
+    block_add(sh_acc, C_EDGES, edges);
+    block_add(sh_acc, C_SECT, sectors);
   }
+}
+
+// Top-down -> top-down: the listed vertices' rows become work items.
+__device__ void chunk_phase(const RunParams& p, const uint2* __restrict__ found_list, int64_t n, TdItem* q_out,
+                            unsigned long long* cnt, unsigned long long* sh_acc) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long skipped = 0;
+  for (;;) {
+    const int64_t base = (int64_t)grab(&cnt[C_WORK]) * 32;
+    if (base >= n) break;
+    const int64_t i = base + lane;
+    uint64_t rb = 0, deg = 0;
+    uint32_t ow = 0;
+    if (i < n) {
+      const uint2 e = __ldcg(found_list + i);
+      rb = __ldg(p.off + e.x);
+      deg = __ldg(p.off + e.x + 1) - rb;
+      ow = e.y;
+      skipped += (deg < 2);
+      if (deg < 2) deg = 0;  // a degree-1 vertex only leads back to its parent
+    }
+    append_row(rb, deg, ow, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
+  }
+  block_add(sh_acc, C_SKIP, skipped);
 }
 
 __device__ __forceinline__ bool vis_test(const uint32_t* __restrict__ vis, uint32_t v) {
   return (__ldg(vis + (v >> 5)) >> (v & 31)) & 1u;
 }
 
-// Bottom-up pass A: every unvisited vertex tests its first neighbour; the
-// misses go to a list for pass B.  BU_WORDS words per warp are in flight.
-__device__ void bu_pass_a(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* __restrict__ vis_next,
-                          uint32_t* __restrict__ miss, unsigned long long* cnt, int64_t lvl) {
+// Bottom-up level: lane l owns vertex l of a 32-vertex word, BU_WORDS words in
+// flight per warp.  First neighbour first; then BU_SERIAL entries alone; the
+// rest of a long row is scanned by the whole warp.
+__device__ void bu_phase(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* __restrict__ vis_next,
+                         unsigned long long* cnt, unsigned long long* sh_acc, int64_t lvl) {
   const int lane = threadIdx.x & 31;
-  unsigned long long found = 0, scanned = 0;
+  unsigned long long found = 0, scanned = 0, edges = 0, sectors = 0;
   for (;;) {
     const int64_t wbase = (int64_t)grab(&cnt[C_WORK]) * 32;
     if (wbase >= p.nwords) break;
@@ -285,131 +333,102 @@ __device__ void bu_pass_a(const RunParams& p, const uint32_t* __restrict__ vis_c
     unsigned todo = __ballot_sync(FULL_MASK, vw != ~0u);
     while (todo) {
       int js[BU_WORDS];
-      uint32_t wv[BU_WORDS], par[BU_WORDS];
+      uint32_t wv[BU_WORDS], parent[BU_WORDS], k[BU_WORDS];
+      uint64_t pos[BU_WORDS], end[BU_WORDS];
 #pragma unroll
       for (int u = 0; u < BU_WORDS; ++u) {
         js[u] = todo ? __ffs(todo) - 1 : -1;
         todo &= todo ? todo - 1 : 0u;
         wv[u] = __shfl_sync(FULL_MASK, vw, js[u] < 0 ? 0 : js[u]);
         if (js[u] < 0) wv[u] = ~0u;
-        par[u] = ((wv[u] >> lane) & 1u) ? NO_VERTEX : __ldg(p.first + (wbase + js[u]) * 32 + lane);
+        parent[u] = ((wv[u] >> lane) & 1u) ? NO_VERTEX : __ldg(p.first + (wbase + js[u]) * 32 + lane);
+        k[u] = 0;
+        pos[u] = end[u] = 0;
       }
-      uint32_t nmiss = 0;
-      unsigned missbits = 0;
 #pragma unroll
       for (int u = 0; u < BU_WORDS; ++u) {
-        const bool active = !((wv[u] >> lane) & 1u);  // every unvisited vertex has an edge
-        const bool hit = active && par[u] != NO_VERTEX && vis_test(vis_cur, par[u]);
-        if (active && !hit) {
-          missbits |= 1u << u;
-          ++nmiss;
+        if (parent[u] != NO_VERTEX) {  // every unvisited vertex has an edge (vertices without one start visited)
+          k[u] = 1;
+          if (!vis_test(vis_cur, parent[u])) {
+            const int64_t v = (wbase + js[u]) * 32 + lane;
+            pos[u] = __ldg(p.off + v) + 1;
+            end[u] = __ldg(p.off + v + 1);
+            parent[u] = NO_VERTEX;
+          }
         }
+      }
+#pragma unroll
+      for (int u = 0; u < BU_WORDS; ++u) {
+        for (int s = 0; s < BU_SERIAL && pos[u] < end[u]; ++s, ++pos[u]) {
+          const uint32_t c = __ldg(p.col + pos[u]);
+          ++k[u];
+          if (vis_test(vis_cur, c)) {
+            parent[u] = c;
+            pos[u] = end[u];
+            break;
+          }
+        }
+        unsigned rest = __ballot_sync(FULL_MASK, pos[u] < end[u]);
+        while (rest) {
+          const int r = __ffs(rest) - 1;
+          rest &= rest - 1;
+          const uint64_t rb = __shfl_sync(FULL_MASK, pos[u], r);
+          const uint64_t re = __shfl_sync(FULL_MASK, end[u], r);
+          uint32_t hitc = NO_VERTEX;
+          uint64_t hitpos = re;
+          for (uint64_t p0 = rb; p0 < re; p0 += 32) {
+            const uint64_t pp = p0 + lane;
+            bool h = false;
+            uint32_t c = 0;
+            if (pp < re) {
+              c = __ldg(p.col + pp);
+              h = vis_test(vis_cur, c);
+            }
+            const unsigned hm = __ballot_sync(FULL_MASK, h);
+            if (hm) {
+              const int hl = __ffs(hm) - 1;
+              hitc = __shfl_sync(FULL_MASK, c, hl);
+              hitpos = p0 + hl;
+              break;
+            }
+          }
+          if (lane == r) {
+            parent[u] = hitc;
+            k[u] += (uint32_t)((hitpos + 1 < re ? hitpos + 1 : re) - rb);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < BU_WORDS; ++u) {
+        if (js[u] < 0) continue;
+        const bool hit = parent[u] != NO_VERTEX;
         const unsigned hits = __ballot_sync(FULL_MASK, hit);
-        if (js[u] >= 0 && lane == 0) {
+        if (lane == 0) {
           vis_next[wbase + js[u]] = wv[u] | hits;
           found += __popc(hits);
           scanned += __popc(~wv[u]);
         }
-        if (hit) p.pred[__ldg(p.invert + (wbase + js[u]) * 32 + lane)] = (int64_t)__ldg(p.invert + par[u]) | lvl;
-      }
-      // misses -> list
-      const uint32_t incl = warp_incl_scan(nmiss);
-      const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
-      if (total) {
-        unsigned long long base = 0;
-        if (lane == 31) base = atomicAdd(&cnt[C_QITEMS], (unsigned long long)total);
-        base = __shfl_sync(FULL_MASK, base, 31) + incl - nmiss;
-#pragma unroll
-        for (int u = 0; u < BU_WORDS; ++u)
-          if (missbits & (1u << u)) miss[base++] = (uint32_t)((wbase + js[u]) * 32 + lane);
-      }
-    }
-  }
-  flush_counter(&cnt[C_DISC], found);
-  flush_counter(&cnt[C_SCAN], scanned);
-  if (p.count_edges) {  // hits examined exactly one edge (one sector)
-    flush_counter(&cnt[C_EDGES], found);
-    flush_counter(&cnt[C_SECT], found);
-  }
-}
-
-// Bottom-up pass B: the rows whose first neighbour missed.  A lane checks
-// BU_SERIAL more entries alone; longer rows are scanned by the whole warp.
-__device__ void bu_pass_b(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* vis_next,
-                          const uint32_t* __restrict__ miss, int64_t nmiss, unsigned long long* cnt, int64_t lvl) {
-  const int lane = threadIdx.x & 31;
-  unsigned long long found = 0, edges = 0, sectors = 0;
-  for (;;) {
-    const int64_t base = (int64_t)grab(&cnt[C_WORK]) * 32;
-    if (base >= nmiss) break;
-    const int64_t i = base + lane;
-    uint32_t v = NO_VERTEX, parent = NO_VERTEX, k = 0;
-    uint64_t pos = 0, end = 0;
-    if (i < nmiss) {
-      v = __ldcg(miss + i);
-      pos = __ldg(p.off + v) + 1;
-      end = __ldg(p.off + v + 1);
-      k = 1;
-      for (int s = 0; s < BU_SERIAL && pos < end; ++s, ++pos) {
-        const uint32_t c = __ldg(p.col + pos);
-        ++k;
-        if (vis_test(vis_cur, c)) {
-          parent = c;
-          pos = end;
-          break;
+        if (hit) p.pred[__ldg(p.invert + (wbase + js[u]) * 32 + lane)] = (int64_t)__ldg(p.invert + parent[u]) | lvl;
+        if (p.count_edges) {
+          edges += k[u];
+          sectors += (k[u] + 7) / 8;
         }
       }
     }
-    unsigned rest = __ballot_sync(FULL_MASK, pos < end);
-    while (rest) {
-      const int r = __ffs(rest) - 1;
-      rest &= rest - 1;
-      const uint64_t rb = __shfl_sync(FULL_MASK, pos, r);
-      const uint64_t re = __shfl_sync(FULL_MASK, end, r);
-      uint32_t hitc = NO_VERTEX;
-      uint64_t hitpos = re;
-      for (uint64_t p0 = rb; p0 < re; p0 += 32) {
-        const uint64_t pp = p0 + lane;
-        bool h = false;
-        uint32_t c = 0;
-        if (pp < re) {
-          c = __ldg(p.col + pp);
-          h = vis_test(vis_cur, c);
-        }
-        const unsigned hm = __ballot_sync(FULL_MASK, h);
-        if (hm) {
-          const int hl = __ffs(hm) - 1;
-          hitc = __shfl_sync(FULL_MASK, c, hl);
-          hitpos = p0 + hl;
-          break;
-        }
-      }
-      if (lane == r) {
-        parent = hitc;
-        k += (uint32_t)((hitpos + 1 < re ? hitpos + 1 : re) - rb);
-      }
-    }
-    if (parent != NO_VERTEX) {
-      atomicOr(vis_next + (v >> 5), 1u << (v & 31));
-      p.pred[__ldg(p.invert + v)] = (int64_t)__ldg(p.invert + parent) | lvl;
-      ++found;
-    }
-    if (p.count_edges && v != NO_VERTEX) {
-      edges += k;
-      sectors += (k + 7) / 8;
-    }
   }
-  flush_counter(&cnt[C_DISC], found);
+  block_add(sh_acc, C_DISC, found);
+  block_add(sh_acc, C_SCAN, scanned);
   if (p.count_edges) {
-    flush_counter(&cnt[C_EDGES], edges);
-    flush_counter(&cnt[C_SECT], sectors);
+    block_add(sh_acc, C_EDGES, edges);
+    block_add(sh_acc, C_SECT, sectors);
   }
 }
 
 // Bottom-up -> top-down: vertices found by the last bottom-up level
 // (vis_new & ~vis_old) become work items.
 __device__ void compact_phase(const RunParams& p, const uint32_t* __restrict__ vis_new,
-                              const uint32_t* __restrict__ vis_old, TdItem* q_out, unsigned long long* cnt) {
+                              const uint32_t* __restrict__ vis_old, TdItem* q_out, unsigned long long* cnt,
+                              unsigned long long* sh_acc) {
   const int lane = threadIdx.x & 31;
   unsigned long long skipped = 0;
   for (;;) {
@@ -432,18 +451,22 @@ __device__ void compact_phase(const RunParams& p, const uint32_t* __restrict__ v
         skipped += (deg < 2);
         if (deg < 2) deg = 0;
       }
-      append_row(rb, deg, ow, true, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
+      append_row(rb, deg, ow, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
     }
   }
-  flush_counter(&cnt[C_SKIP], skipped);
+  block_add(sh_acc, C_SKIP, skipped);
 }
 
-__global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(RunParams p) {
+__global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_kernel(RunParams p) {
   __shared__ unsigned long long sh_cnt[C_NUM];
+  __shared__ unsigned long long sh_acc[C_NUM];
   __shared__ unsigned sh_flag;
   BfsCtl* ctl = p.ctl;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  TdItem* items = p.queue[0];
+  uint2* found_list = reinterpret_cast<uint2*>(p.queue[1]);
+  if (threadIdx.x < C_NUM) sh_acc[threadIdx.x] = 0;
 
   // initialize_memory (bfs.hpp:241-276): pred = -1, visited = ~has_edge
   if (tid == 0) ctl->t0_ns = globaltimer();
@@ -455,7 +478,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(RunParam
   const uint64_t root_b = has_edges ? p.off[root_r] : 0;
   const uint64_t root_deg = has_edges ? p.off[root_r + 1] - root_b : 0;
   const int64_t root_items = (int64_t)chunks_of(root_deg);
-  if (!grid_sync(ctl, nullptr, sh_cnt, &sh_flag)) return;
+  if (!grid_sync(ctl, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
 
   // first_expand (bfs.hpp:477-518): the root's row becomes the first queue
   for (int64_t c = tid; c < root_items; c += nthreads) {
@@ -464,7 +487,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(RunParam
     it.orig = (uint32_t)p.root;
     const uint64_t left = root_deg - (uint64_t)c * TD_CHUNK;
     it.len = (uint32_t)(left < (uint64_t)TD_CHUNK ? left : (uint64_t)TD_CHUNK) | (c == 0 ? FIRST_CHUNK : 0u);
-    p.queue[0][c] = it;
+    items[c] = it;
   }
   if (tid == 0) {
     p.pred[p.root] = p.root;
@@ -479,60 +502,38 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(RunParam
     }
     return;
   }
-  if (!grid_sync(ctl, nullptr, sh_cnt, &sh_flag)) return;
+  if (!grid_sync(ctl, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
   if (tid == 0) ctl->t_init_ns = globaltimer();
 
-  int cur_vis = 0, cur_q = 0;
+  int cur_vis = 0;
   bool forward = true, growing = true;
   int64_t qn = root_items, prev_nq = 0, visited = 1, carried = 0;
   unsigned phase = 0;
   int level = 1;
+  // Each phase uses counter slot phase%3 and clears slot (phase+1)%3 for the
+  // next one; a slot is read right after its phase's barrier, so it is never
+  // cleared while a block may still read it.
+#define NEXT_PHASE_SLOT()                                                              \
+  (blockIdx.x == 0 && threadIdx.x < C_NUM ? (void)(ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0) : (void)0), \
+      ctl->cnt[phase % 3]
   for (;; ++level) {
-    unsigned long long* cnt = ctl->cnt[phase % 3];
-    if (blockIdx.x == 0 && threadIdx.x < C_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
+    unsigned long long* cnt = (NEXT_PHASE_SLOT());
     const int64_t lvl = (int64_t)level << 48;
-    unsigned long long disc = 0, scan = 0, edges = 0, sect = 0, front = 0, skip = 0, qitems = 0;
-    if (forward) {
-      td_phase(p, p.queue[cur_q], qn, p.vis[cur_vis], p.queue[cur_q ^ 1], cnt, lvl);
-      if (!grid_sync(ctl, cnt, sh_cnt, &sh_flag)) return;
-      ++phase;
-      disc = sh_cnt[C_DISC];
-      edges = sh_cnt[C_EDGES];
-      sect = sh_cnt[C_SECT];
-      front = sh_cnt[C_FRONT];
-      skip = sh_cnt[C_SKIP];
-      qitems = sh_cnt[C_QITEMS];
-    } else {
-      uint32_t* miss = reinterpret_cast<uint32_t*>(p.queue[0]);
-      bu_pass_a(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, cnt, lvl);
-      if (!grid_sync(ctl, cnt, sh_cnt, &sh_flag)) return;
-      ++phase;
-      disc = sh_cnt[C_DISC];
-      scan = sh_cnt[C_SCAN];
-      edges = sh_cnt[C_EDGES];
-      sect = sh_cnt[C_SECT];
-      const int64_t nmiss = (int64_t)sh_cnt[C_QITEMS];
-      if (nmiss > 0) {
-        unsigned long long* cnt_b = ctl->cnt[phase % 3];
-        if (blockIdx.x == 0 && threadIdx.x < C_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
-        bu_pass_b(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, nmiss, cnt_b, lvl);
-        if (!grid_sync(ctl, cnt_b, sh_cnt, &sh_flag)) return;
-        ++phase;
-        disc += sh_cnt[C_DISC];
-        edges += sh_cnt[C_EDGES];
-        sect += sh_cnt[C_SECT];
-      }
-    }
-    const int64_t nq = (int64_t)disc;
+    if (forward) td_phase(p, items, qn, p.vis[cur_vis], found_list, cnt, sh_acc, lvl);
+    else bu_phase(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], cnt, sh_acc, lvl);
+    if (!grid_sync(ctl, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
+    ++phase;
+    const int64_t nq = (int64_t)sh_cnt[C_DISC];
+    const int64_t listed = (int64_t)sh_cnt[C_QITEMS];
     if (tid == 0) {
       LevelRecord r;
       r.direction = forward ? 1 : 0;
       r.level = level;
-      r.frontier = forward ? front + carried : 0;
-      r.discovered = disc;
-      r.scanned = scan;
-      r.edges = edges + (forward ? carried : 0);
-      r.sectors = sect + (forward ? carried : 0);
+      r.frontier = forward ? sh_cnt[C_FRONT] + carried : 0;
+      r.discovered = nq;
+      r.scanned = sh_cnt[C_SCAN];
+      r.edges = sh_cnt[C_EDGES] + (forward ? carried : 0);
+      r.sectors = sh_cnt[C_SECT] + (forward ? carried : 0);
       r.t_ns = globaltimer();
       p.rec[level - 1] = r;
     }
@@ -553,25 +554,20 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) bfs_persistent_kernel(RunParam
     }
     prev_nq = nq;
     if (forward) {
-      if (was_forward) {
-        cur_q ^= 1;
-        qn = (int64_t)qitems;
-        carried = (int64_t)skip;
-      } else {
-        unsigned long long* ccnt = ctl->cnt[phase % 3];
-        if (blockIdx.x == 0 && threadIdx.x < C_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
-        compact_phase(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], p.queue[cur_q], ccnt);
-        if (!grid_sync(ctl, ccnt, sh_cnt, &sh_flag)) return;
-        ++phase;
-        qn = (int64_t)sh_cnt[C_QITEMS];
-        carried = (int64_t)sh_cnt[C_SKIP];
-      }
+      unsigned long long* ccnt = (NEXT_PHASE_SLOT());
+      if (was_forward) chunk_phase(p, found_list, listed, items, ccnt, sh_acc);
+      else compact_phase(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], items, ccnt, sh_acc);
+      if (!grid_sync(ctl, ccnt, sh_acc, ccnt, sh_cnt, &sh_flag)) return;
+      ++phase;
+      qn = (int64_t)sh_cnt[C_QITEMS];
+      carried = (int64_t)sh_cnt[C_SKIP];
       if (qn > p.cap) {  // append_row already flagged it; never read past the queue
         if (tid == 0) atomicOr(&ctl->err, (unsigned)BFS_ERR_QUEUE);
         return;
       }
     }
   }
+#undef NEXT_PHASE_SLOT
   if (tid == 0) {
     ctl->num_levels = (unsigned)level;
     ctl->final_vis = cur_vis;
@@ -641,8 +637,8 @@ extern "C" int g500_bfs_create(g500_graph* g, g500_bfs** out) {
   if (st == G500_OK) st = dev_alloc_n(&b->d_pred, g->nolv, "pred");
   if (st == G500_OK) st = dev_alloc_n(&b->d_vis[0], nwords, "visited bitmap");
   if (st == G500_OK) st = dev_alloc_n(&b->d_vis[1], nwords, "visited bitmap");
-  if (st == G500_OK) st = dev_alloc_n(&b->d_queue[0], b->queue_cap, "top-down queue / bottom-up miss list");
-  if (st == G500_OK) st = dev_alloc_n(&b->d_queue[1], b->queue_cap, "top-down queue");
+  if (st == G500_OK) st = dev_alloc_n(&b->d_queue[0], b->queue_cap, "top-down work items");
+  if (st == G500_OK) st = dev_alloc_n(&b->d_queue[1], b->queue_cap, "top-down discovered list");
   if (st == G500_OK) st = dev_alloc_n(&b->d_ctl, 1, "bfs control block");
   if (st == G500_OK) st = dev_alloc_n(&b->d_rec, MAX_LEVELS, "level records");
   if (st == G500_OK) chk(cudaHostAlloc(&b->h_ctl, sizeof(BfsCtl), cudaHostAllocDefault), "cudaHostAlloc");
