@@ -38,9 +38,9 @@
 namespace g500 {
 
 constexpr int BFS_THREADS = 256;
-constexpr int BFS_MIN_BLOCKS = 3;        // co-resident blocks per SM (80 registers, no spills)
+constexpr int BFS_MIN_BLOCKS = 4;        // co-resident blocks per SM (64 registers, no spills)
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
-constexpr int BU_WORDS = 4;               // 32-vertex words a warp keeps in flight
+constexpr int BU_WORDS = 8;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
 constexpr int BU_SERIAL = 6;              // row entries a lane checks alone before the warp helps
 constexpr unsigned long long SPIN_LIMIT = 1ull << 25;  // ~ seconds of __nanosleep(64)
 
@@ -104,11 +104,24 @@ __device__ __forceinline__ void flush_counter(unsigned long long* c, unsigned lo
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(c, v);
 }
 
-// next dynamically scheduled batch index of this warp
-__device__ __forceinline__ unsigned long long grab(unsigned long long* work) {
-  unsigned long long b = 0;
-  if ((threadIdx.x & 31) == 0) b = atomicAdd(work, 1ull);
-  return __shfl_sync(FULL_MASK, b, 0);
+__device__ __forceinline__ int64_t gwarp_id() { return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ int64_t gwarp_count() { return ((int64_t)gridDim.x * blockDim.x) >> 5; }
+
+// position of the r-th (0-based) set bit of m (m has more than r set bits)
+__device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t r) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (int w = 16; w; w >>= 1) {
+    const uint32_t lo = __popc(m & ((1u << w) - 1u));
+    if (r >= lo) {
+      r -= lo;
+      m >>= w;
+      pos += w;
+    } else {
+      m &= (1u << w) - 1u;
+    }
+  }
+  return pos;
 }
 
 // Add a warp's value to the block accumulator of counter i (flushed to the
@@ -131,7 +144,6 @@ __device__ bool grid_sync(BfsCtl* ctl, unsigned long long* flush_slot, unsigned 
     const unsigned long long v = sh_acc[threadIdx.x];
     if (flush_slot && v) atomicAdd(&flush_slot[threadIdx.x], v);
     sh_acc[threadIdx.x] = 0;
-    __threadfence();
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -213,13 +225,11 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
                          uint2* __restrict__ found_list, unsigned long long* cnt, unsigned long long* sh_acc,
                          int64_t lvl) {
   const int lane = threadIdx.x & 31;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t nwarps = gwarp_count();
   const int64_t per_warp = (qn + nwarps - 1) / nwarps;
   const int B = per_warp >= 32 ? 32 : (per_warp < 1 ? 1 : (int)per_warp);  // items per batch
   unsigned long long found = 0, frontier = 0, edges = 0, sectors = 0;
-  for (;;) {
-    const int64_t base = (int64_t)grab(&cnt[C_WORK]) * B;
-    if (base >= qn) break;
+  for (int64_t base = gwarp_id() * B; base < qn; base += nwarps * B) {
     const int64_t qi = base + lane;
     uint64_t b = 0;
     uint32_t len = 0, orig_u = 0;
@@ -294,9 +304,7 @@ __device__ void chunk_phase(const RunParams& p, const uint2* __restrict__ found_
                             unsigned long long* cnt, unsigned long long* sh_acc) {
   const int lane = threadIdx.x & 31;
   unsigned long long skipped = 0;
-  for (;;) {
-    const int64_t base = (int64_t)grab(&cnt[C_WORK]) * 32;
-    if (base >= n) break;
+  for (int64_t base = gwarp_id() * 32; base < n; base += gwarp_count() * 32) {
     const int64_t i = base + lane;
     uint64_t rb = 0, deg = 0;
     uint32_t ow = 0;
@@ -317,107 +325,137 @@ __device__ __forceinline__ bool vis_test(const uint32_t* __restrict__ vis, uint3
   return (__ldg(vis + (v >> 5)) >> (v & 31)) & 1u;
 }
 
-// Bottom-up level: lane l owns vertex l of a 32-vertex word, BU_WORDS words in
-// flight per warp.  First neighbour first; then BU_SERIAL entries alone; the
-// rest of a long row is scanned by the whole warp.
-__device__ void bu_phase(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* __restrict__ vis_next,
-                         unsigned long long* cnt, unsigned long long* sh_acc, int64_t lvl) {
+// Bottom-up pass A: lane l owns vertex l of a 32-vertex word, BU_WORDS words
+// in flight per warp.  Each unvisited vertex tests its first (smallest
+// reordered id; under VERTEX_REORDERING=2 the highest-degree) neighbour -- the
+// reference's isolated first edge.  New bits come from one ballot per word
+// (no atomics); the vertices that missed are marked in a miss bitmap.
+__device__ void bu_pass_a(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* __restrict__ vis_next,
+                          uint32_t* __restrict__ miss, unsigned long long* sh_acc, int64_t lvl) {
   const int lane = threadIdx.x & 31;
-  unsigned long long found = 0, scanned = 0, edges = 0, sectors = 0;
-  for (;;) {
-    const int64_t wbase = (int64_t)grab(&cnt[C_WORK]) * 32;
-    if (wbase >= p.nwords) break;
+  unsigned long long found = 0, scanned = 0, nmiss = 0;
+  for (int64_t wbase = gwarp_id() * 32; wbase < p.nwords; wbase += gwarp_count() * 32) {
     const int64_t wi = wbase + lane;
     const uint32_t vw = wi < p.nwords ? __ldg(vis_cur + wi) : ~0u;
-    if (wi < p.nwords && vw == ~0u) vis_next[wi] = vw;
+    if (wi < p.nwords && vw == ~0u) {
+      vis_next[wi] = vw;
+      miss[wi] = 0;
+    }
     unsigned todo = __ballot_sync(FULL_MASK, vw != ~0u);
     while (todo) {
       int js[BU_WORDS];
-      uint32_t wv[BU_WORDS], parent[BU_WORDS], k[BU_WORDS];
-      uint64_t pos[BU_WORDS], end[BU_WORDS];
+      uint32_t wv[BU_WORDS], pf[BU_WORDS];
 #pragma unroll
       for (int u = 0; u < BU_WORDS; ++u) {
         js[u] = todo ? __ffs(todo) - 1 : -1;
         todo &= todo ? todo - 1 : 0u;
         wv[u] = __shfl_sync(FULL_MASK, vw, js[u] < 0 ? 0 : js[u]);
         if (js[u] < 0) wv[u] = ~0u;
-        parent[u] = ((wv[u] >> lane) & 1u) ? NO_VERTEX : __ldg(p.first + (wbase + js[u]) * 32 + lane);
-        k[u] = 0;
-        pos[u] = end[u] = 0;
+        pf[u] = ((wv[u] >> lane) & 1u) ? NO_VERTEX : __ldg(p.first + (wbase + js[u]) * 32 + lane);
       }
 #pragma unroll
       for (int u = 0; u < BU_WORDS; ++u) {
-        if (parent[u] != NO_VERTEX) {  // every unvisited vertex has an edge (vertices without one start visited)
-          k[u] = 1;
-          if (!vis_test(vis_cur, parent[u])) {
-            const int64_t v = (wbase + js[u]) * 32 + lane;
-            pos[u] = __ldg(p.off + v) + 1;
-            end[u] = __ldg(p.off + v + 1);
-            parent[u] = NO_VERTEX;
-          }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < BU_WORDS; ++u) {
-        for (int s = 0; s < BU_SERIAL && pos[u] < end[u]; ++s, ++pos[u]) {
-          const uint32_t c = __ldg(p.col + pos[u]);
-          ++k[u];
-          if (vis_test(vis_cur, c)) {
-            parent[u] = c;
-            pos[u] = end[u];
-            break;
-          }
-        }
-        unsigned rest = __ballot_sync(FULL_MASK, pos[u] < end[u]);
-        while (rest) {
-          const int r = __ffs(rest) - 1;
-          rest &= rest - 1;
-          const uint64_t rb = __shfl_sync(FULL_MASK, pos[u], r);
-          const uint64_t re = __shfl_sync(FULL_MASK, end[u], r);
-          uint32_t hitc = NO_VERTEX;
-          uint64_t hitpos = re;
-          for (uint64_t p0 = rb; p0 < re; p0 += 32) {
-            const uint64_t pp = p0 + lane;
-            bool h = false;
-            uint32_t c = 0;
-            if (pp < re) {
-              c = __ldg(p.col + pp);
-              h = vis_test(vis_cur, c);
-            }
-            const unsigned hm = __ballot_sync(FULL_MASK, h);
-            if (hm) {
-              const int hl = __ffs(hm) - 1;
-              hitc = __shfl_sync(FULL_MASK, c, hl);
-              hitpos = p0 + hl;
-              break;
-            }
-          }
-          if (lane == r) {
-            parent[u] = hitc;
-            k[u] += (uint32_t)((hitpos + 1 < re ? hitpos + 1 : re) - rb);
-          }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < BU_WORDS; ++u) {
-        if (js[u] < 0) continue;
-        const bool hit = parent[u] != NO_VERTEX;
+        const bool active = !((wv[u] >> lane) & 1u);  // every unvisited vertex has an edge
+        const bool hit = active && pf[u] != NO_VERTEX && vis_test(vis_cur, pf[u]);
         const unsigned hits = __ballot_sync(FULL_MASK, hit);
-        if (lane == 0) {
+        const unsigned misses = __ballot_sync(FULL_MASK, active && !hit);
+        if (js[u] >= 0 && lane == 0) {
           vis_next[wbase + js[u]] = wv[u] | hits;
+          miss[wbase + js[u]] = misses;
           found += __popc(hits);
           scanned += __popc(~wv[u]);
+          nmiss += __popc(misses);
         }
-        if (hit) p.pred[__ldg(p.invert + (wbase + js[u]) * 32 + lane)] = (int64_t)__ldg(p.invert + parent[u]) | lvl;
-        if (p.count_edges) {
-          edges += k[u];
-          sectors += (k[u] + 7) / 8;
-        }
+        if (hit) p.pred[__ldg(p.invert + (wbase + js[u]) * 32 + lane)] = (int64_t)__ldg(p.invert + pf[u]) | lvl;
       }
     }
   }
   block_add(sh_acc, C_DISC, found);
   block_add(sh_acc, C_SCAN, scanned);
+  block_add(sh_acc, C_QITEMS, nmiss);
+  if (p.count_edges) {  // a first-neighbour hit examined one edge (one sector)
+    block_add(sh_acc, C_EDGES, found);
+    block_add(sh_acc, C_SECT, found);
+  }
+}
+
+// Bottom-up pass B: the vertices whose first neighbour missed.  Each warp
+// gathers 32 of them into its lanes; a lane checks BU_SERIAL more row entries
+// alone, and rows still unresolved are scanned by the whole warp.
+__device__ void bu_pass_b(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* vis_next,
+                          const uint32_t* __restrict__ miss, unsigned long long* sh_acc, int64_t lvl) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long found = 0, edges = 0, sectors = 0;
+  for (int64_t wbase = gwarp_id() * 32; wbase < p.nwords; wbase += gwarp_count() * 32) {
+    const int64_t wi = wbase + lane;
+    const uint32_t mw = wi < p.nwords ? __ldcg(miss + wi) : 0u;
+    const uint32_t c = __popc(mw);
+    const uint32_t incl = warp_incl_scan(c);
+    const uint32_t excl = incl - c;
+    const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
+    for (uint32_t b0 = 0; b0 < total; b0 += 32) {
+      const uint32_t idx = b0 + lane;
+      const int o = owner_lane(excl, idx);
+      const uint32_t mwo = __shfl_sync(FULL_MASK, mw, o);
+      const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
+      uint32_t v = NO_VERTEX, parent = NO_VERTEX, k = 0;
+      uint64_t pos = 0, end = 0;
+      if (idx < total) {
+        v = (uint32_t)((wbase + o) * 32 + select_bit(mwo, idx - exo));
+        pos = __ldg(p.off + v) + 1;
+        end = __ldg(p.off + v + 1);
+        k = 1;
+        for (int s = 0; s < BU_SERIAL && pos < end; ++s, ++pos) {
+          const uint32_t cv = __ldg(p.col + pos);
+          ++k;
+          if (vis_test(vis_cur, cv)) {
+            parent = cv;
+            pos = end;
+            break;
+          }
+        }
+      }
+      unsigned rest = __ballot_sync(FULL_MASK, pos < end);
+      while (rest) {
+        const int r = __ffs(rest) - 1;
+        rest &= rest - 1;
+        const uint64_t rb = __shfl_sync(FULL_MASK, pos, r);
+        const uint64_t re = __shfl_sync(FULL_MASK, end, r);
+        uint32_t hitc = NO_VERTEX;
+        uint64_t hitpos = re;
+        for (uint64_t p0 = rb; p0 < re; p0 += 32) {
+          const uint64_t pp = p0 + lane;
+          bool h = false;
+          uint32_t cv = 0;
+          if (pp < re) {
+            cv = __ldg(p.col + pp);
+            h = vis_test(vis_cur, cv);
+          }
+          const unsigned hm = __ballot_sync(FULL_MASK, h);
+          if (hm) {
+            const int hl = __ffs(hm) - 1;
+            hitc = __shfl_sync(FULL_MASK, cv, hl);
+            hitpos = p0 + hl;
+            break;
+          }
+        }
+        if (lane == r) {
+          parent = hitc;
+          k += (uint32_t)((hitpos + 1 < re ? hitpos + 1 : re) - rb);
+        }
+      }
+      if (parent != NO_VERTEX) {
+        atomicOr(vis_next + (v >> 5), 1u << (v & 31));
+        p.pred[__ldg(p.invert + v)] = (int64_t)__ldg(p.invert + parent) | lvl;
+        ++found;
+      }
+      if (p.count_edges && v != NO_VERTEX) {
+        edges += k;
+        sectors += (k + 7) / 8;
+      }
+    }
+  }
+  block_add(sh_acc, C_DISC, found);
   if (p.count_edges) {
     block_add(sh_acc, C_EDGES, edges);
     block_add(sh_acc, C_SECT, sectors);
@@ -431,9 +469,7 @@ __device__ void compact_phase(const RunParams& p, const uint32_t* __restrict__ v
                               unsigned long long* sh_acc) {
   const int lane = threadIdx.x & 31;
   unsigned long long skipped = 0;
-  for (;;) {
-    const int64_t wbase = (int64_t)grab(&cnt[C_WORK]) * 32;
-    if (wbase >= p.nwords) break;
+  for (int64_t wbase = gwarp_id() * 32; wbase < p.nwords; wbase += gwarp_count() * 32) {
     const int64_t wi = wbase + lane;
     const uint32_t f = wi < p.nwords ? (__ldcg(vis_new + wi) & ~__ldcg(vis_old + wi)) : 0u;
     unsigned todo = __ballot_sync(FULL_MASK, f != 0);
@@ -519,21 +555,45 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   for (;; ++level) {
     unsigned long long* cnt = (NEXT_PHASE_SLOT());
     const int64_t lvl = (int64_t)level << 48;
-    if (forward) td_phase(p, items, qn, p.vis[cur_vis], found_list, cnt, sh_acc, lvl);
-    else bu_phase(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], cnt, sh_acc, lvl);
-    if (!grid_sync(ctl, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
-    ++phase;
-    const int64_t nq = (int64_t)sh_cnt[C_DISC];
-    const int64_t listed = (int64_t)sh_cnt[C_QITEMS];
+    unsigned long long disc, scan = 0, edges, sect, front = 0, listed = 0;
+    if (forward) {
+      td_phase(p, items, qn, p.vis[cur_vis], found_list, cnt, sh_acc, lvl);
+      if (!grid_sync(ctl, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
+      ++phase;
+      disc = sh_cnt[C_DISC];
+      edges = sh_cnt[C_EDGES];
+      sect = sh_cnt[C_SECT];
+      front = sh_cnt[C_FRONT];
+      listed = sh_cnt[C_QITEMS];
+    } else {
+      uint32_t* miss = reinterpret_cast<uint32_t*>(found_list);
+      bu_pass_a(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, sh_acc, lvl);
+      if (!grid_sync(ctl, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
+      ++phase;
+      disc = sh_cnt[C_DISC];
+      scan = sh_cnt[C_SCAN];
+      edges = sh_cnt[C_EDGES];
+      sect = sh_cnt[C_SECT];
+      if (sh_cnt[C_QITEMS] > 0) {  // some first neighbours missed
+        unsigned long long* cnt_b = (NEXT_PHASE_SLOT());
+        bu_pass_b(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, sh_acc, lvl);
+        if (!grid_sync(ctl, cnt_b, sh_acc, cnt_b, sh_cnt, &sh_flag)) return;
+        ++phase;
+        disc += sh_cnt[C_DISC];
+        edges += sh_cnt[C_EDGES];
+        sect += sh_cnt[C_SECT];
+      }
+    }
+    const int64_t nq = (int64_t)disc;
     if (tid == 0) {
       LevelRecord r;
       r.direction = forward ? 1 : 0;
       r.level = level;
-      r.frontier = forward ? sh_cnt[C_FRONT] + carried : 0;
-      r.discovered = nq;
-      r.scanned = sh_cnt[C_SCAN];
-      r.edges = sh_cnt[C_EDGES] + (forward ? carried : 0);
-      r.sectors = sh_cnt[C_SECT] + (forward ? carried : 0);
+      r.frontier = forward ? front + carried : 0;
+      r.discovered = disc;
+      r.scanned = scan;
+      r.edges = edges + (forward ? carried : 0);
+      r.sectors = sect + (forward ? carried : 0);
       r.t_ns = globaltimer();
       p.rec[level - 1] = r;
     }
@@ -555,7 +615,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
     prev_nq = nq;
     if (forward) {
       unsigned long long* ccnt = (NEXT_PHASE_SLOT());
-      if (was_forward) chunk_phase(p, found_list, listed, items, ccnt, sh_acc);
+      if (was_forward) chunk_phase(p, found_list, (int64_t)listed, items, ccnt, sh_acc);
       else compact_phase(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], items, ccnt, sh_acc);
       if (!grid_sync(ctl, ccnt, sh_acc, ccnt, sh_cnt, &sh_flag)) return;
       ++phase;
