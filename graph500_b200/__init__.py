@@ -48,7 +48,8 @@ class GraphInfo(C.Structure):
 class LevelStats(C.Structure):
     _fields_ = [("direction", C.c_int32), ("level", C.c_int32), ("frontier", C.c_int64),
                 ("discovered", C.c_int64), ("scanned", C.c_int64), ("edge_sectors", C.c_int64),
-                ("edges_examined", C.c_int64), ("device_ms", C.c_double)]
+                ("edges_examined", C.c_int64), ("device_ms", C.c_double),
+                ("device_ms_tail", C.c_double)]
 
 
 class BfsStats(C.Structure):

@@ -493,6 +493,23 @@ __device__ void compact_phase(const RunParams& p, const uint32_t* __restrict__ v
   block_add(sh_acc, C_SKIP, skipped);
 }
 
+__device__ __forceinline__ void write_record(LevelRecord* rec, int level, bool td, unsigned long long frontier,
+                                             unsigned long long disc, unsigned long long scan,
+                                             unsigned long long edges, unsigned long long sect,
+                                             unsigned long long t_mid) {
+  LevelRecord r;
+  r.direction = td ? 1 : 0;
+  r.level = level;
+  r.frontier = td ? frontier : 0;
+  r.discovered = disc;
+  r.scanned = scan;
+  r.edges = edges;
+  r.sectors = sect;
+  r.t_mid_ns = t_mid;
+  r.t_ns = globaltimer();
+  rec[level - 1] = r;
+}
+
 __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_kernel(RunParams p) {
   __shared__ unsigned long long sh_cnt[C_NUM];
   __shared__ unsigned long long sh_acc[C_NUM];
@@ -555,10 +572,11 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   for (;; ++level) {
     unsigned long long* cnt = (NEXT_PHASE_SLOT());
     const int64_t lvl = (int64_t)level << 48;
-    unsigned long long disc, scan = 0, edges, sect, front = 0, listed = 0;
+    unsigned long long disc, scan = 0, edges, sect, front = 0, listed = 0, t_mid = 0;
     if (forward) {
       td_phase(p, items, qn, p.vis[cur_vis], found_list, cnt, sh_acc, lvl);
       if (!grid_sync(ctl, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
+      if (tid == 0) t_mid = globaltimer();
       ++phase;
       disc = sh_cnt[C_DISC];
       edges = sh_cnt[C_EDGES];
@@ -569,6 +587,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       uint32_t* miss = reinterpret_cast<uint32_t*>(found_list);
       bu_pass_a(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, sh_acc, lvl);
       if (!grid_sync(ctl, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
+      if (tid == 0) t_mid = globaltimer();
       ++phase;
       disc = sh_cnt[C_DISC];
       scan = sh_cnt[C_SCAN];
@@ -585,22 +604,15 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       }
     }
     const int64_t nq = (int64_t)disc;
-    if (tid == 0) {
-      LevelRecord r;
-      r.direction = forward ? 1 : 0;
-      r.level = level;
-      r.frontier = forward ? front + carried : 0;
-      r.discovered = disc;
-      r.scanned = scan;
-      r.edges = edges + (forward ? carried : 0);
-      r.sectors = sect + (forward ? carried : 0);
-      r.t_ns = globaltimer();
-      p.rec[level - 1] = r;
-    }
+    const int64_t carried_in = carried;
     visited += nq;
     const bool was_forward = forward;
     if (!forward) cur_vis ^= 1;  // the bottom-up output is the current visited map
-    if (nq == 0) break;
+    if (nq == 0) {
+      if (tid == 0) write_record(p.rec, level, was_forward, front + carried_in, disc, scan,
+                                 edges + (was_forward ? carried_in : 0), sect + (was_forward ? carried_in : 0), t_mid);
+      break;
+    }
     if (level >= MAX_LEVELS) {
       if (tid == 0) atomicOr(&ctl->err, (unsigned)BFS_ERR_DEPTH);
       break;
@@ -626,6 +638,9 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
         return;
       }
     }
+    if (tid == 0)
+      write_record(p.rec, level, was_forward, front + carried_in, disc, scan,
+                   edges + (was_forward ? carried_in : 0), sect + (was_forward ? carried_in : 0), t_mid);
   }
 #undef NEXT_PHASE_SLOT
   if (tid == 0) {
@@ -839,6 +854,7 @@ extern "C" int g500_bfs_level_stats(const g500_bfs* b, g500_level_stats* out, in
     o.edges_examined = (int64_t)r.edges;
     o.edge_sectors = (int64_t)r.sectors;
     o.device_ms = (double)(r.t_ns - prev) * 1e-6;  // %globaltimer between level barriers
+    o.device_ms_tail = r.t_mid_ns ? (double)(r.t_ns - r.t_mid_ns) * 1e-6 : 0.0;
     prev = r.t_ns;
   }
   return G500_OK;

@@ -142,7 +142,8 @@ struct LevelRecord {
   int32_t direction;
   int32_t level;
   unsigned long long frontier, discovered, scanned, edges, sectors;
-  unsigned long long t_ns;  // %globaltimer when the level's barrier completed
+  unsigned long long t_mid_ns;  // %globaltimer after the level's first barrier (TD expand / BU pass A)
+  unsigned long long t_ns;      // %globaltimer when the level's last barrier completed
 };
 
 constexpr int MAX_LEVELS = 0xFFFE;

@@ -125,7 +125,8 @@ typedef struct g500_level_stats {
   int64_t scanned;         /* BU: unvisited vertices with edges scanned */
   int64_t edge_sectors;    /* TD: sum ceil(deg/8); BU: sum ceil(k/8) (if counting on) */
   int64_t edges_examined;  /* TD: sum deg; BU: sum k (if counting on) */
-  double device_ms;        /* CUDA-event time of this level's kernels */
+  double device_ms;        /* device time of the level (%globaltimer between level barriers) */
+  double device_ms_tail;   /* part after the level's first barrier: BU miss pass / TD row chunking */
 } g500_level_stats;
 
 typedef struct g500_bfs_stats {
