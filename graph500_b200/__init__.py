@@ -129,8 +129,30 @@ def _ptr(obj) -> tuple[int, bool]:
         return obj.ctypes.data, False
     cai = getattr(obj, "__cuda_array_interface__", None)
     if cai is not None:
+        if cai.get("strides") not in (None, ()):
+            raise ValueError("CUDA array must be contiguous")
         return int(cai["data"][0]), True
     raise TypeError(f"unsupported buffer type {type(obj)!r}")
+
+
+def _nbytes(obj) -> int:
+    """Size in bytes of a numpy array or a contiguous CUDA array."""
+    if isinstance(obj, np.ndarray):
+        return obj.nbytes
+    cai = obj.__cuda_array_interface__
+    n = 1
+    for d in cai["shape"]:
+        n *= int(d)
+    return n * int(np.dtype(cai["typestr"]).itemsize)
+
+
+def _num_edges(edges) -> int:
+    """Packed 12-byte edges held by a buffer (the count is derived from its
+    byte size, never from its element count)."""
+    nb = _nbytes(edges)
+    if nb % EDGE_DTYPE.itemsize:
+        raise ValueError(f"edge buffer of {nb} bytes is not a whole number of 12-byte packed edges")
+    return nb // EDGE_DTYPE.itemsize
 
 
 # ---------------------------------------------------------------------------
@@ -160,6 +182,8 @@ def generate_edges(scale: int, edgefactor: int = 16, start: int = 0, end: int | 
     if out is None:
         out = np.zeros(end - start, dtype=EDGE_DTYPE)
     ptr, dev = _ptr(out)
+    if _nbytes(out) < (end - start) * EDGE_DTYPE.itemsize:
+        raise ValueError("output buffer too small for the requested edge range")
     check(lib().g500_gen_edges(scale, edgefactor, seed1, seed2, start, end, ptr, int(dev), None))
     return out
 
@@ -196,7 +220,7 @@ class Graph2DCSR:
     def build(cls, edges: np.ndarray, reorder_mode: int = 2, keep_edges: bool = True, device: int = 0):
         ptr, dev = _ptr(edges)
         h = C.c_void_p()
-        check(lib().g500_graph_build(ptr, len(edges), int(dev), reorder_mode, int(keep_edges), device,
+        check(lib().g500_graph_build(ptr, _num_edges(edges), int(dev), reorder_mode, int(keep_edges), device,
                                      C.byref(h)))
         return cls(h.value)
 
@@ -303,6 +327,8 @@ class BfsOnGPU:
         if self.h is None:
             raise G500Error(G500_E_STATE, "prepare_bfs() first")
         ptr, dev = _ptr(pred)
+        if _nbytes(pred) < 8 * self.graph_.pred_size():
+            raise ValueError(f"pred holds fewer than pred_size() = {self.graph_.pred_size()} int64 entries")
         st = BfsStats()
         check(lib().g500_bfs_run(self.h, int(root), ptr, int(dev), C.byref(st)))
         self.last_stats = st
@@ -348,11 +374,13 @@ def validate_bfs_result(graph: Graph2DCSR, root: int, pred, edge_list=None) -> t
     edge list.  Returns (ok, edge_visit_count, per-stage error counts).
     """
     pptr, pdev = _ptr(pred)
+    if _nbytes(pred) < 8 * graph.pred_size():
+        raise ValueError(f"pred holds fewer than pred_size() = {graph.pred_size()} int64 entries")
     eptr, edev, m = None, 1, 0
     if edge_list is not None:
         edges = edge_list.edges if isinstance(edge_list, EdgeList) else edge_list
         eptr, d = _ptr(edges)
-        edev, m = int(d), len(edges)
+        edev, m = int(d), _num_edges(edges)
     evc, ok, rep = C.c_int64(), C.c_int(), ValidateReport()
     check(lib().g500_validate(graph.h, eptr, m, edev, int(root), pptr, int(pdev), C.byref(evc), C.byref(ok),
                               C.byref(rep)))

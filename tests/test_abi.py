@@ -71,3 +71,21 @@ def test_product_does_not_reference_oracle():
             if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp", ".cc")):
                 text = open(os.path.join(dirpath, f)).read()
                 assert "import oracle" not in text and "liboracle" not in text and "g500_oracle" not in text, f
+
+
+class _FakeCudaArray:
+    """An object exposing __cuda_array_interface__ (no GPU memory behind it)."""
+
+    def __init__(self, shape, typestr):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (0, False), "version": 3,
+                                         "strides": None}
+
+
+def test_edge_count_comes_from_byte_size(g500):
+    """A 3*m int32 device buffer holds m packed edges, not 3*m."""
+    assert g500._num_edges(_FakeCudaArray((30,), "<i4")) == 10
+    assert g500._num_edges(_FakeCudaArray((5, 3), "<u4")) == 5
+    import numpy as np
+    assert g500._num_edges(np.zeros(7, g500.EDGE_DTYPE)) == 7
+    with pytest.raises(ValueError):
+        g500._num_edges(_FakeCudaArray((31,), "<i4"))
