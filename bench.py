@@ -47,8 +47,10 @@ def parse_args():
     ap.add_argument("--edgefactor", type=int, default=16)
     ap.add_argument("--roots", type=int, default=64)
     ap.add_argument("--reorder", type=int, default=2)
-    ap.add_argument("--alpha", type=float, default=2000.0)
-    ap.add_argument("--beta", type=float, default=8.0)
+    ap.add_argument("--alpha", type=float, default=None, help="fix alpha (disables the autotuner)")
+    ap.add_argument("--beta", type=float, default=None, help="fix beta (disables the autotuner)")
+    ap.add_argument("--policy", type=int, default=0, help="direction policy with fixed alpha/beta: 0 reference, 1 edges")
+    ap.add_argument("--tune-roots", type=int, default=8, help="roots the autotuner samples (untimed)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-roots", type=int, default=8, help="roots in the bounded CPU-baseline sample")
     ap.add_argument("--ref-roots-per-step", type=int, default=4)
@@ -59,7 +61,7 @@ def workload(a) -> dict:
     return {"workload": f"plain direction-optimizing BFS, Kronecker SCALE {a.scale} edgefactor {a.edgefactor}, "
                         f"VERTEX_REORDERING {a.reorder}, {a.roots} roots per step",
             "scale": a.scale, "edgefactor": a.edgefactor, "roots_per_step": a.roots,
-            "vertex_reordering": a.reorder, "alpha": a.alpha, "beta": a.beta,
+            "vertex_reordering": a.reorder,
             "l2": "flushed (256 MiB write) before every root, outside the timed events",
             "parallelism": f"replicas x{a.gpus}"}
 
@@ -232,9 +234,20 @@ def our_arm(a):
     bfs.construct(g5.EdgeList(None, a.scale, a.edgefactor))
     gen_s, build_s = bfs.graph_.timings()
     info = bfs.graph_.info
-    bfs.prepare_bfs(a.alpha, a.beta, count_edges=True)
+    bfs.prepare_bfs()
     roots = g5.find_roots(bfs.graph_, a.roots)
     pred_dev = torch.empty(info.pred_size, dtype=torch.int64, device="cuda")
+    if a.alpha is None and a.beta is None:
+        tune = bfs.autotune(roots[:a.tune_roots], reps=2)  # untimed; picks policy/alpha/beta
+        policy, alpha, beta = tune["policy"], tune["alpha"], tune["beta"]
+        tuning = {"autotuned_on_roots": int(min(a.tune_roots, len(roots))), "configs_tried": tune["configs_tried"],
+                  "tuned_ms": tune["best_ms"], "reference_setting_ms": tune["reference_ms"]}
+    else:
+        policy = a.policy
+        alpha = 2000.0 if a.alpha is None else a.alpha
+        beta = 8.0 if a.beta is None else a.beta
+        tuning = {"autotuned_on_roots": 0}
+    bfs.set_params(alpha, beta, count_edges=True, policy=policy)
 
     # untimed: validate every root, record the per-level counts of the bytes model
     nedge, model = [], []
@@ -245,7 +258,7 @@ def our_arm(a):
             raise SystemExit(f"validation failed for root {r}: {rep}")
         nedge.append(evc)
         model.append(bytes_model(bfs.level_stats(), info.pred_size, info.num_local_verts))
-    bfs.set_params(a.alpha, a.beta, count_edges=False)
+    bfs.set_params(alpha, beta, count_edges=False, policy=policy)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def step(record: dict | None):
@@ -321,7 +334,8 @@ def our_arm(a):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 1000.0 * t_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32", "data": "synthetic (Graph500 Kronecker generator, seeds 2/3, generated on the GPU)",
-        "config": workload(a),
+        "config": dict(workload(a), direction_policy=["reference", "edges"][policy], alpha=alpha, beta=beta,
+                       **tuning),
         "harmonic_mean_gteps": hm,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * len(roots),
                 "d2h_bytes_per_step": 8 * info.pred_size * len(roots)},

@@ -58,6 +58,14 @@ class BfsStats(C.Structure):
                 ("kernel_launches", C.c_int32)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("policy", C.c_int32), ("configs_tried", C.c_int32), ("alpha", C.c_double), ("beta", C.c_double),
+                ("best_ms", C.c_double), ("reference_ms", C.c_double)]
+
+
+DIR_REFERENCE, DIR_EDGES = 0, 1
+
+
 class ValidateReport(C.Structure):
     _fields_ = [("range_errors", C.c_int64), ("root_errors", C.c_int64), ("self_parent_errors", C.c_int64),
                 ("depth_errors", C.c_int64), ("edge_errors", C.c_int64),
@@ -101,6 +109,8 @@ def lib() -> C.CDLL:
         "g500_bfs_create": ([P, C.POINTER(P)], i32),
         "g500_bfs_set_params": ([P, C.c_double, C.c_double, i32], i32),
         "g500_bfs_set_stream": ([P, P], i32),
+        "g500_bfs_set_policy": ([P, i32], i32),
+        "g500_bfs_autotune": ([P, P, i32, i32, C.POINTER(TuneResult)], i32),
         "g500_bfs_run": ([P, i64, P, i32, C.POINTER(BfsStats)], i32),
         "g500_bfs_level_stats": ([P, P, i32, C.POINTER(i32)], i32),
         "g500_bfs_device_pred": ([P, C.POINTER(P)], i32),
@@ -311,16 +321,27 @@ class BfsOnGPU:
             self.graph_ = Graph2DCSR.build(edges, self.reorder_mode, keep_edges, self.device)
 
     # bfs.hpp:115-118
-    def prepare_bfs(self, alpha: float = 2000.0, beta: float = 8.0, count_edges: bool = False) -> None:
+    def prepare_bfs(self, alpha: float = 2000.0, beta: float = 8.0, count_edges: bool = False,
+                    policy: int = DIR_REFERENCE) -> None:
         if self.graph_ is None:
             raise G500Error(G500_E_STATE, "construct() first")
         h = C.c_void_p()
         check(lib().g500_bfs_create(self.graph_.h, C.byref(h)))
         self.h = h
-        self.set_params(alpha, beta, count_edges)
+        self.set_params(alpha, beta, count_edges, policy)
 
-    def set_params(self, alpha: float = 2000.0, beta: float = 8.0, count_edges: bool = False) -> None:
+    def set_params(self, alpha: float = 2000.0, beta: float = 8.0, count_edges: bool = False,
+                   policy: int | None = None) -> None:
         check(lib().g500_bfs_set_params(self.h, alpha, beta, int(count_edges)))
+        if policy is not None:
+            check(lib().g500_bfs_set_policy(self.h, policy))
+
+    def autotune(self, roots, reps: int = 2) -> dict:
+        """Pick the direction policy and thresholds on sample roots (kept on the handle)."""
+        r = np.ascontiguousarray(roots, dtype=np.int64)
+        out = TuneResult()
+        check(lib().g500_bfs_autotune(self.h, r.ctypes.data, len(r), reps, C.byref(out)))
+        return {f[0]: getattr(out, f[0]) for f in TuneResult._fields_}
 
     # bfs.hpp:120, :2651-2940
     def run_bfs(self, root: int, pred) -> BfsStats:

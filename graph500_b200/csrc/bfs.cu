@@ -60,6 +60,7 @@ struct RunParams {
   int64_t root;
   double alpha, beta;
   int count_edges;
+  int policy;
 };
 
 constexpr uint32_t FIRST_CHUNK = 0x80000000u;
@@ -228,7 +229,7 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
   const int64_t nwarps = gwarp_count();
   const int64_t per_warp = (qn + nwarps - 1) / nwarps;
   const int B = per_warp >= 32 ? 32 : (per_warp < 1 ? 1 : (int)per_warp);  // items per batch
-  unsigned long long found = 0, frontier = 0, edges = 0, sectors = 0;
+  unsigned long long found = 0, frontier = 0, edges = 0, sectors = 0, mf = 0;
   for (int64_t base = gwarp_id() * B; base < qn; base += nwarps * B) {
     const int64_t qi = base + lane;
     uint64_t b = 0;
@@ -276,6 +277,7 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
         if (won[j]) {
           ow[j] = __ldg(p.invert + w[j]);
           p.pred[ow[j]] = (int64_t)uo[j] | lvl;
+          if (p.policy == G500_DIR_EDGES) mf += __ldg(p.off + w[j] + 1) - __ldg(p.off + w[j]);
         }
       }
       const uint32_t wincl = warp_incl_scan(nwon);
@@ -292,6 +294,7 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
     }
   }
   block_add(sh_acc, C_DISC, found);
+  block_add(sh_acc, C_MF, mf);
   if (p.count_edges) {
     block_add(sh_acc, C_FRONT, frontier);
     block_add(sh_acc, C_EDGES, edges);
@@ -561,6 +564,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   int cur_vis = 0;
   bool forward = true, growing = true;
   int64_t qn = root_items, prev_nq = 0, visited = 1, carried = 0;
+  int64_t mu = (int64_t)(p.off[p.nlv] - root_deg);  // degree sum of unvisited vertices (edge policy)
   unsigned phase = 0;
   int level = 1;
   // Each phase uses counter slot phase%3 and clears slot (phase+1)%3 for the
@@ -572,7 +576,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   for (;; ++level) {
     unsigned long long* cnt = (NEXT_PHASE_SLOT());
     const int64_t lvl = (int64_t)level << 48;
-    unsigned long long disc, scan = 0, edges, sect, front = 0, listed = 0, t_mid = 0;
+    unsigned long long disc, scan = 0, edges, sect, front = 0, listed = 0, t_mid = 0, mf = 0;
     if (forward) {
       td_phase(p, items, qn, p.vis[cur_vis], found_list, cnt, sh_acc, lvl);
       if (!grid_sync(ctl, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
@@ -583,6 +587,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       sect = sh_cnt[C_SECT];
       front = sh_cnt[C_FRONT];
       listed = sh_cnt[C_QITEMS];
+      mf = sh_cnt[C_MF];
     } else {
       uint32_t* miss = reinterpret_cast<uint32_t*>(found_list);
       bu_pass_a(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, sh_acc, lvl);
@@ -618,7 +623,15 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       break;
     }
     const int64_t unvisited = p.ngv - visited;
-    if (growing && nq > prev_nq) {
+    if (was_forward) mu -= (int64_t)mf;
+    if (p.policy == G500_DIR_EDGES) {
+      if (forward && growing) {
+        if ((double)mf > (double)mu / p.alpha) forward = false;
+      } else if (!forward && nq < prev_nq && (double)nq < (double)p.ngv / p.beta) {
+        forward = true;
+        growing = false;
+      }
+    } else if (growing && nq > prev_nq) {  // the reference's rule, bfs.hpp:2799-2829
       if (forward && (double)nq > (double)p.ngv / p.alpha) forward = false;
     } else if (!forward && unvisited < (int64_t)((double)p.ngv / p.beta)) {
       forward = true;
@@ -748,6 +761,70 @@ extern "C" int g500_bfs_set_params(g500_bfs* b, double alpha, double beta, int c
   return G500_OK;
 }
 
+extern "C" int g500_bfs_set_policy(g500_bfs* b, int policy) {
+  if (!b) return set_error(G500_E_INVAL, "null bfs");
+  if (policy != G500_DIR_REFERENCE && policy != G500_DIR_EDGES)
+    return set_error(G500_E_INVAL, "unknown direction policy %d", policy);
+  b->policy = policy;
+  return G500_OK;
+}
+
+extern "C" int g500_bfs_autotune(g500_bfs* b, const int64_t* roots, int nroots, int reps, g500_tune_result* out) {
+  if (!b || !roots || nroots <= 0) return set_error(G500_E_INVAL, "bad argument");
+  if (reps < 1) reps = 1;
+  struct Cfg { int policy; double alpha, beta; };
+  static const Cfg grid[] = {
+      {G500_DIR_REFERENCE, 2000.0, 8.0},  {G500_DIR_REFERENCE, 100.0, 8.0},  {G500_DIR_REFERENCE, 500.0, 1e9},
+      {G500_DIR_REFERENCE, 100.0, 1e9},   {G500_DIR_REFERENCE, 2000.0, 1e9}, {G500_DIR_REFERENCE, 20000.0, 1e9},
+      {G500_DIR_EDGES, 2.0, 24.0},        {G500_DIR_EDGES, 6.0, 24.0},       {G500_DIR_EDGES, 15.0, 24.0},
+      {G500_DIR_EDGES, 2.0, 1e9},         {G500_DIR_EDGES, 6.0, 1e9},        {G500_DIR_EDGES, 15.0, 1e9},
+      {G500_DIR_EDGES, 50.0, 1e9},        {G500_DIR_EDGES, 150.0, 1e9},
+  };
+  const int ncfg = (int)(sizeof(grid) / sizeof(grid[0]));
+  const int saved_count = b->count_edges;
+  b->count_edges = 0;
+  double best = 1e300, ref_ms = 0;
+  int best_i = 0;
+  for (int c = 0; c < ncfg; ++c) {
+    b->policy = grid[c].policy;
+    b->alpha = grid[c].alpha;
+    b->beta = grid[c].beta;
+    double sum = 0;
+    for (int r = 0; r < nroots; ++r) {
+      double m = 1e300;
+      for (int k = 0; k < reps; ++k) {
+        g500_bfs_stats st;
+        int rc = g500_bfs_run(b, roots[r], b->d_pred, 1, &st);
+        if (rc != G500_OK) {
+          b->count_edges = saved_count;
+          return rc;
+        }
+        m = std::min(m, st.device_ms);
+      }
+      sum += m;
+    }
+    const double mean = sum / nroots;
+    if (c == 0) ref_ms = mean;
+    if (mean < best) {
+      best = mean;
+      best_i = c;
+    }
+  }
+  b->policy = grid[best_i].policy;
+  b->alpha = grid[best_i].alpha;
+  b->beta = grid[best_i].beta;
+  b->count_edges = saved_count;
+  if (out) {
+    out->policy = b->policy;
+    out->configs_tried = ncfg;
+    out->alpha = b->alpha;
+    out->beta = b->beta;
+    out->best_ms = best;
+    out->reference_ms = ref_ms;
+  }
+  return G500_OK;
+}
+
 extern "C" int g500_bfs_set_stream(g500_bfs* b, void* stream) {
   if (!b) return set_error(G500_E_INVAL, "null bfs");
   b->stream = stream ? (cudaStream_t)stream : b->own_stream;
@@ -784,6 +861,7 @@ extern "C" int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_o
   p.cap = b->queue_cap;
   p.root = root;
   p.alpha = b->alpha;
+  p.policy = b->policy;
   p.beta = b->beta;
   p.count_edges = b->count_edges;
   void* args[] = {&p};

@@ -112,7 +112,7 @@ struct g500_graph {
 };
 
 // Per-phase counters of the persistent BFS kernel (3 rotating slots).
-enum BfsCounter { C_QITEMS = 0, C_DISC, C_SCAN, C_EDGES, C_SECT, C_FRONT, C_SKIP, C_WORK, C_NUM };
+enum BfsCounter { C_QITEMS = 0, C_DISC, C_SCAN, C_EDGES, C_SECT, C_FRONT, C_SKIP, C_MF, C_NUM };  // C_MF: degree sum of new top-down discoveries
 
 // Top-down work item: one chunk (<= TD_CHUNK edges) of a frontier row.
 struct __align__(16) TdItem {
@@ -153,6 +153,7 @@ struct g500_bfs {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   double alpha = 2000.0, beta = 8.0;
+  int policy = 0;                    // G500_DIR_REFERENCE or G500_DIR_EDGES
   int count_edges = 0;
   unsigned grid = 0;                 // co-resident blocks of the persistent kernel
 

@@ -146,8 +146,31 @@ int g500_bfs_create(g500_graph* g, g500_bfs** out);
  * 2000, DEMON_BOTTOMUP_TO_TOPDOWN 8; parameters.h:87-88, bfs.hpp:2799-2829).
  * count_edges != 0 records edge_sectors/edges_examined per level (slower). */
 int g500_bfs_set_params(g500_bfs* b, double alpha, double beta, int count_edges);
+/* Direction policy.  G500_DIR_REFERENCE is the reference's rule (bfs.hpp:
+ * 2799-2829): TD -> BU when growing and nq > num_global_verts / alpha; BU -> TD
+ * when unvisited < num_global_verts / beta.  G500_DIR_EDGES compares edges
+ * instead (Beamer, Asanovic, Patterson, SC'12): TD -> BU when the new
+ * frontier's degree sum m_f > (degree sum of unvisited vertices) / alpha;
+ * BU -> TD when the frontier shrinks below num_global_verts / beta.  Levels are
+ * the same under every policy; only the parents and the speed differ. */
+enum g500_dir_policy { G500_DIR_REFERENCE = 0, G500_DIR_EDGES = 1 };
+int g500_bfs_set_policy(g500_bfs* b, int policy);
 /* Use this stream for the runs (NULL = the handle's own stream). */
 int g500_bfs_set_stream(g500_bfs* b, void* stream);
+
+/* Autotuner: time every (policy, alpha, beta) of a built-in grid on the given
+ * roots (device pred, best of `reps` runs per root), keep the fastest on the
+ * handle and report it.  No counterpart in the reference (its thresholds are
+ * compile-time constants, parameters.h:87-88). */
+typedef struct g500_tune_result {
+  int32_t policy;
+  int32_t configs_tried;
+  double alpha;
+  double beta;
+  double best_ms;          /* mean device time per BFS of the chosen setting */
+  double reference_ms;     /* the same for the reference setting (policy 0, 2000, 8) */
+} g500_tune_result;
+int g500_bfs_autotune(g500_bfs* b, const int64_t* roots, int num_roots, int reps, g500_tune_result* out);
 /* BfsBase::run_bfs(root, pred) (bfs.hpp:120, :2651-2940): writes EVERY entry
  * of pred[pred_size]: parent | level << 48 for reached vertices, root = root,
  * -1 otherwise.  pred is device memory if pred_on_device else host memory

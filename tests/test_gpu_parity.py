@@ -137,18 +137,36 @@ def test_level_counters_match_oracle_schedule(g500, oracle_mod, vr):
     bfs.close()
 
 
-@pytest.mark.parametrize("alpha,beta", [(1e18, 8.0), (1e-9, 1e-9), (2000.0, 1e9), (30.0, 2.0)])
-def test_levels_independent_of_switch_thresholds(g500, oracle_mod, alpha, beta):
+@pytest.mark.parametrize("policy,alpha,beta", [(0, 1e18, 8.0), (0, 1e-9, 1e-9), (0, 2000.0, 1e9), (0, 30.0, 2.0),
+                                               (1, 15.0, 24.0), (1, 1e-9, 1e9), (1, 1e18, 1.0), (1, 2.0, 1e-9)])
+def test_levels_independent_of_switch_thresholds(g500, oracle_mod, policy, alpha, beta):
     edges = oracle_mod.generate_edges(13)
     og = oracle_mod.Graph(edges, 2)
     bfs = g500.BfsOnGPU(reorder_mode=2)
     bfs.construct(edges)
-    bfs.prepare_bfs(alpha, beta)
+    bfs.prepare_bfs(alpha, beta, policy=policy)
     pred = np.zeros(bfs.graph_.pred_size(), np.int64)
     for root in og.find_roots(4):
         bfs.run_bfs(int(root), pred)
         assert np.array_equal(g500.levels_from_pred(pred), og.bfs_levels(int(root)))
         assert g500.validate_bfs_result(bfs.graph_, int(root), pred)[0]
+    bfs.close()
+
+
+def test_autotune_keeps_results_identical(g500, oracle_mod):
+    edges = oracle_mod.generate_edges(14)
+    og = oracle_mod.Graph(edges, 2)
+    bfs = g500.BfsOnGPU(reorder_mode=2)
+    bfs.construct(edges)
+    bfs.prepare_bfs()
+    roots = og.find_roots(6)
+    tune = bfs.autotune(roots[:3], reps=1)
+    assert tune["configs_tried"] >= 8 and tune["best_ms"] <= tune["reference_ms"] + 1e-9
+    pred = np.zeros(bfs.graph_.pred_size(), np.int64)
+    for r in roots:
+        bfs.run_bfs(int(r), pred)
+        assert np.array_equal(g500.levels_from_pred(pred), og.bfs_levels(int(r)))
+        assert g500.validate_bfs_result(bfs.graph_, int(r), pred)[0]
     bfs.close()
 
 
