@@ -181,6 +181,22 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def traffic_per_bfs(a):
+    """DRAM bytes of one bfs_persistent_kernel launch from the committed ncu
+    summary for this workload (profiles/bfs_persistent_kernel_s<SCALE>.md,
+    line 'traffic_per_launch_bytes: N'), or None when there is none."""
+    p = os.path.join(ROOT, "profiles", f"bfs_persistent_kernel_s{a.scale}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("traffic_per_launch_bytes:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
 def bytes_model(levels, pred_size, nlv):
     """Algorithmic bytes of one BFS: 8 B per pred entry, and per level
     TD: 32 B per frontier vertex (offsets) + 32 B per adjacency sector + 32 B per discovered vertex;
@@ -325,11 +341,12 @@ def our_arm(a):
         return
 
     peak, peak_kind = load_peaks()
-    dom = "bu" if rec["bu_ms"] >= rec["td_ms"] else "td"
-    dom_bytes = rec[dom + "_bytes"] / max(rec[dom + "_launches"], 1)
-    dom_ms = rec[dom + "_ms"] / max(rec[dom + "_launches"], 1)
-    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9 if dom_ms > 0 else 0.0
-    whole = (rec["td_bytes"] + rec["bu_bytes"] + rec["pred_bytes"]) / (sum(rec["t"]) / 1000.0) / 1e9
+    # One persistent kernel runs a whole BFS, so it is the dominant kernel:
+    # algorithmic bytes of one BFS / its mean device time.
+    runs = len(rec["t"])
+    bytes_per_bfs = (rec["td_bytes"] + rec["bu_bytes"] + rec["pred_bytes"]) / runs
+    ms_per_bfs = sum(rec["t"]) / runs
+    achieved = bytes_per_bfs / (ms_per_bfs / 1000.0) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 1000.0 * t_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -340,11 +357,12 @@ def our_arm(a):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * len(roots),
                 "d2h_bytes_per_step": 8 * info.pred_size * len(roots)},
         "gpu_launches": rec["launches"],
-        "roofline": {"bound": "hbm", "kernel": f"{dom}_kernel", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                     "whole_bfs_achieved": whole, "whole_bfs_frac": whole / peak,
-                     "bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
-                     "level_ms": {"td": rec["td_ms"] / len(rec["t"]), "bu": rec["bu_ms"] / len(rec["t"])}},
+        "roofline": {"bound": "hbm", "kernel": "bfs_persistent_kernel", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_per_bfs(a),
+                     "bytes_per_launch": bytes_per_bfs, "ms_per_launch": ms_per_bfs,
+                     "bytes_split": {"pred": rec["pred_bytes"] / runs, "top_down": rec["td_bytes"] / runs,
+                                     "bottom_up": rec["bu_bytes"] / runs},
+                     "level_ms": {"top_down": rec["td_ms"] / runs, "bottom_up": rec["bu_ms"] / runs}},
         "clocks": clocks,
         "graph": {"num_global_verts": info.num_global_verts, "num_global_edges": info.num_global_edges,
                   "pred_size": info.pred_size, "nedge_per_root": int(statistics.median(nedge)),
