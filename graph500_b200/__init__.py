@@ -117,6 +117,8 @@ def lib() -> C.CDLL:
         "g500_bfs_destroy": ([P], i32),
         "g500_validate": ([P, P, i64, i32, i64, P, i32, C.POINTER(i64), C.POINTER(i32), C.POINTER(ValidateReport)],
                           i32),
+        "g500_validate_noalloc": ([P, i64, i64, i64, i64, P, P, C.POINTER(i64), C.POINTER(i32),
+                                   C.POINTER(ValidateReport)], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

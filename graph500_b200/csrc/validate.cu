@@ -16,6 +16,7 @@
 #include "g500_internal.cuh"
 
 #include <algorithm>
+#include <mutex>
 
 namespace g500 {
 
@@ -174,6 +175,92 @@ extern "C" int g500_validate(g500_graph* g, const g500_packed_edge* edges, int64
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   cleanup();
   if (e != cudaSuccess) return cuda_error(e, "validation", __FILE__, __LINE__);
+  g500_validate_report r;
+  r.range_errors = (int64_t)h[VE_RANGE];
+  r.root_errors = (int64_t)h[VE_ROOT];
+  r.self_parent_errors = (int64_t)h[VE_SELF];
+  r.depth_errors = (int64_t)h[VE_DEPTH];
+  r.edge_errors = (int64_t)h[VE_EDGE];
+  r.missing_parent_edge_errors = (int64_t)h[VE_MISSING];
+  const bool valid = !(r.range_errors || r.root_errors || r.self_parent_errors || r.depth_errors ||
+                       r.edge_errors || r.missing_parent_edge_errors);
+  *ok = valid ? 1 : 0;
+  if (edge_visit_count) *edge_visit_count = valid ? (int64_t)h[VE_COUNT_EDGES] : 0;
+  if (report) *report = r;
+  return G500_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Validation that allocates nothing.
+//
+// Some callers cannot call cudaMalloc: a host framework that owns all device
+// memory through its own arena or caching allocator, or a serving loop that
+// forbids allocation once it has started.  For them the scratch of the
+// validator (one flag byte per vertex and the error counters) lives in
+// file-scope device arrays of a fixed size, held by every GPU that loads the
+// library until the process exits.  Host code cannot use the arrays' names as
+// device addresses, so each device's addresses are fetched once with
+// cudaGetSymbolAddress, with that device current.
+// ---------------------------------------------------------------------------
+namespace g500 {
+
+static __device__ __align__(256) uint8_t g_static_valid[G500_VALIDATE_STATIC_MAX_VERTS];
+static __device__ __align__(256) unsigned long long g_static_err[VE_N];
+
+struct StaticScratch {
+  uint8_t* valid = nullptr;
+  unsigned long long* err = nullptr;
+};
+static StaticScratch g_static_scratch[64];
+static std::mutex g_static_mu;
+
+// Resolve this device's scratch addresses (first call on a device only).
+static int static_scratch(int dev, StaticScratch* out) {
+  if (dev < 0 || dev >= 64) return set_error(G500_E_INVAL, "device %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  StaticScratch& s = g_static_scratch[dev];
+  if (!s.valid) {
+    void* v = nullptr;
+    void* e = nullptr;
+    G500_CUDA(cudaGetSymbolAddress(&v, g_static_valid));
+    G500_CUDA(cudaGetSymbolAddress(&e, g_static_err));
+    s.valid = static_cast<uint8_t*>(v);
+    s.err = static_cast<unsigned long long*>(e);
+  }
+  *out = s;
+  return G500_OK;
+}
+
+}  // namespace g500
+
+extern "C" int g500_validate_noalloc(const g500_packed_edge* dev_edges, int64_t num_edges, int64_t nglobalverts,
+                                     int64_t nlocalverts, int64_t root, const int64_t* dev_pred, void* stream,
+                                     int64_t* edge_visit_count, int* ok, g500_validate_report* report) {
+  if (!dev_pred || !ok || (num_edges > 0 && !dev_edges)) return set_error(G500_E_INVAL, "null argument");
+  if (num_edges < 0 || nlocalverts <= 0 || nglobalverts < 0 || nglobalverts > nlocalverts)
+    return set_error(G500_E_INVAL, "bad sizes (num_edges %lld, nglobalverts %lld, nlocalverts %lld)",
+                     (long long)num_edges, (long long)nglobalverts, (long long)nlocalverts);
+  if (nlocalverts > G500_VALIDATE_STATIC_MAX_VERTS)
+    return set_error(G500_E_RANGE, "g500_validate_noalloc handles at most %d vertices (pred_size %lld); "
+                     "use g500_validate", G500_VALIDATE_STATIC_MAX_VERTS, (long long)nlocalverts);
+  int dev = 0;
+  G500_CUDA(cudaGetDevice(&dev));
+  StaticScratch sc;
+  G500_TRY(static_scratch(dev, &sc));
+  cudaStream_t s = (cudaStream_t)stream;
+  // the arrays keep the last call's contents: clear what must start at zero
+  G500_CUDA(cudaMemsetAsync(sc.err, 0, sizeof(unsigned long long) * VE_N, s));
+  G500_CUDA(cudaMemsetAsync(sc.valid, 0, (size_t)nlocalverts, s));
+  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(std::max<int64_t>(nlocalverts, num_edges), 256),
+                                                    (int64_t)num_sms() * 16);
+  val_root_kernel<<<1, 1, 0, s>>>(dev_pred, root, nlocalverts, sc.err);
+  val_vertex_kernel<<<grid, 256, 0, s>>>(dev_pred, nlocalverts, nglobalverts, root, sc.err);
+  if (num_edges > 0) val_edge_kernel<<<grid, 256, 0, s>>>(dev_edges, num_edges, dev_pred, nlocalverts, sc.valid, sc.err);
+  val_parent_kernel<<<grid, 256, 0, s>>>(dev_pred, nlocalverts, root, sc.valid, sc.err);
+  G500_CUDA(cudaGetLastError());
+  unsigned long long h[VE_N];
+  G500_CUDA(cudaMemcpyAsync(h, sc.err, sizeof(h), cudaMemcpyDeviceToHost, s));
+  G500_CUDA(cudaStreamSynchronize(s));
   g500_validate_report r;
   r.range_errors = (int64_t)h[VE_RANGE];
   r.root_errors = (int64_t)h[VE_ROOT];

@@ -202,6 +202,26 @@ int g500_validate(g500_graph* g, const g500_packed_edge* edges, int64_t num_edge
                   int edges_on_device, int64_t root, const int64_t* pred, int pred_on_device,
                   int64_t* edge_visit_count, int* ok, g500_validate_report* report);
 
+/* Validation that allocates nothing, for callers that cannot call cudaMalloc
+ * (a host framework owning all device memory through its own arena or caching
+ * allocator, or a serving loop that forbids allocation after start-up).  No
+ * counterpart in the reference.  Same checks and results as g500_validate,
+ * with every buffer passed by the caller in device memory (edges, pred) and
+ * nglobalverts / nlocalverts given explicitly (main.cc:129-133 passes
+ * max_used_vertex + 1 and pred_size).  Scratch is a fixed device array of
+ * G500_VALIDATE_STATIC_MAX_VERTS bytes plus a few counters, held by every GPU
+ * that loads the library until the process exits; larger nlocalverts is
+ * refused with G500_E_RANGE.  The first call on a device resolves that
+ * device's scratch address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  Every call shares the same scratch: calls that overlap
+ * on the GPU (e.g. on two streams) race and must be serialised by the caller.
+ * stream may be NULL (the default stream); the call returns after the stream
+ * has finished the validation. */
+#define G500_VALIDATE_STATIC_MAX_VERTS (1 << 22)
+int g500_validate_noalloc(const g500_packed_edge* dev_edges, int64_t num_edges, int64_t nglobalverts,
+                          int64_t nlocalverts, int64_t root, const int64_t* dev_pred, void* stream,
+                          int64_t* edge_visit_count, int* ok, g500_validate_report* report);
+
 #ifdef __cplusplus
 }
 #endif
