@@ -210,6 +210,44 @@ def bytes_model(levels, pred_size, nlv):
     return 8 * pred_size, td, bu
 
 
+def batched_arm(a, g5, torch, bfs, roots, nedge, pred_dev, local, reduce_max, reduce_sum, barrier) -> dict:
+    """MS-BFS over the same roots: autotune (untimed), check every root's levels
+    against the plain BFS (untimed), then time K launches of all roots."""
+    ms = g5.MultiSourceBFS(bfs.graph_, 64, 15.0, True)
+    r = np.asarray(roots, dtype=np.int64)
+    tune = ms.autotune(r, reps=1)
+    out = torch.empty((len(r), bfs.graph_.pred_size()), dtype=torch.uint8, device="cuda")
+    ms.run(r, out)
+    for i, root in enumerate(r):
+        bfs.run_bfs(int(root), pred_dev)
+        lv = ((pred_dev >> 48) & 0xFFFF)
+        lv = torch.where(pred_dev == -1, torch.full_like(lv, 255), lv).to(torch.uint8)
+        if not torch.equal(lv, out[i]):
+            raise SystemExit(f"batched levels differ from the plain BFS for root {root}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(a.warmup):
+        ms.run(r)
+    t = 0.0
+    levels = pulls = 0
+    barrier()
+    for _ in range(a.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        st = ms.run(r)
+        t += st.device_ms
+        levels, pulls = st.num_levels, st.pull_levels
+    barrier()
+    t_max = reduce_max(t / 1000.0)
+    e_all = reduce_sum(float(a.steps * sum(nedge)))
+    ms.close()
+    return {"metric": "aggregate GTEPS of batched multi-source BFS (same graph, same roots)",
+            "value": e_all / t_max / 1e9, "unit": UNIT, "roots_per_launch": int(min(len(r), tune["lane_width"])),
+            "roots": int(len(r)), "lane_width": tune["lane_width"], "alpha": tune["alpha"],
+            "ms_per_step": 1000.0 * t_max / a.steps, "levels": levels, "pull_levels": pulls,
+            "output": "uint8 level array per root in original-id order, on the device",
+            "parity": "levels of every root equal the plain BFS's (pred >> 48)"}
+
+
 def our_arm(a):
     import torch
 
@@ -334,6 +372,9 @@ def our_arm(a):
     e2e_value = e_all / e2e_max / 1e9
     g5.check(g5.lib().g500_host_free(hp))
 
+    # batched multi-source BFS on the same graph and roots (one launch per 64 roots)
+    batched = batched_arm(a, g5, torch, bfs, roots, nedge, pred_dev, local, reduce_max, reduce_sum, barrier)
+
     if rank != 0:
         bfs.close()
         if dist:
@@ -368,6 +409,8 @@ def our_arm(a):
                   "pred_size": info.pred_size, "nedge_per_root": int(statistics.median(nedge)),
                   "generation_s": gen_s, "construction_s": build_s, "setup_wall_s": time.time() - t0},
     }
+    line["batched"] = batched
+    line["batched"]["speedup_vs_plain"] = batched["value"] / value if value else None
     if world == 1 and not a.no_cpu_baseline:
         crec, err = run_ref_bench(a.scale, a.edgefactor, a.cpu_roots, 0, 1, a.cpu_roots, a.reorder)
         if crec is not None:

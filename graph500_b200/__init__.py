@@ -66,6 +66,17 @@ class TuneResult(C.Structure):
 DIR_REFERENCE, DIR_EDGES = 0, 1
 
 
+class MsStats(C.Structure):
+    _fields_ = [("device_ms", C.c_double), ("host_ms", C.c_double), ("num_levels", C.c_int32),
+                ("pull_levels", C.c_int32), ("lane_width", C.c_int32), ("batches", C.c_int32),
+                ("kernel_launches", C.c_int32), ("pad", C.c_int32)]
+
+
+class MsTune(C.Structure):
+    _fields_ = [("lane_width", C.c_int32), ("configs_tried", C.c_int32), ("alpha", C.c_double),
+                ("best_ms", C.c_double)]
+
+
 class ValidateReport(C.Structure):
     _fields_ = [("range_errors", C.c_int64), ("root_errors", C.c_int64), ("self_parent_errors", C.c_int64),
                 ("depth_errors", C.c_int64), ("edge_errors", C.c_int64),
@@ -117,6 +128,13 @@ def lib() -> C.CDLL:
         "g500_bfs_destroy": ([P], i32),
         "g500_validate": ([P, P, i64, i32, i64, P, i32, C.POINTER(i64), C.POINTER(i32), C.POINTER(ValidateReport)],
                           i32),
+        "g500_msbfs_create": ([P, C.POINTER(P)], i32),
+        "g500_msbfs_set_params": ([P, i32, C.c_double, i32], i32),
+        "g500_msbfs_run": ([P, P, i32, P, i32, C.POINTER(MsStats)], i32),
+        "g500_msbfs_root_stats": ([P, P, P], i32),
+        "g500_msbfs_device_levels": ([P, C.POINTER(P)], i32),
+        "g500_msbfs_autotune": ([P, P, i32, i32, C.POINTER(MsTune)], i32),
+        "g500_msbfs_destroy": ([P], i32),
         "g500_validate_noalloc": ([P, i64, i64, i64, i64, P, P, C.POINTER(i64), C.POINTER(i32),
                                    C.POINTER(ValidateReport)], i32),
     }
@@ -384,6 +402,65 @@ class BfsOnGPU:
         if self.graph_ is not None:
             self.graph_.close()
             self.graph_ = None
+
+
+# ---------------------------------------------------------------------------
+# batched multi-source BFS
+# ---------------------------------------------------------------------------
+class MultiSourceBFS:
+    """Many roots per launch (bit-lanes of 32/64/128-bit masks per vertex)."""
+
+    def __init__(self, graph: Graph2DCSR, lane_width: int = 64, alpha: float = 15.0, use_cuda_graph: bool = True):
+        self.graph = graph
+        h = C.c_void_p()
+        check(lib().g500_msbfs_create(graph.h, C.byref(h)))
+        self.h = h
+        self.set_params(lane_width, alpha, use_cuda_graph)
+
+    def set_params(self, lane_width: int = 64, alpha: float = 15.0, use_cuda_graph: bool = True) -> None:
+        check(lib().g500_msbfs_set_params(self.h, lane_width, alpha, int(use_cuda_graph)))
+
+    def run(self, roots, levels=None) -> MsStats:
+        """levels: None (stay on the device), or a host/device buffer of
+        len(roots) * pred_size bytes (root-major, 255 = unreached)."""
+        r = np.ascontiguousarray(roots, dtype=np.int64)
+        st = MsStats()
+        if levels is None:
+            check(lib().g500_msbfs_run(self.h, r.ctypes.data, len(r), None, 0, C.byref(st)))
+        else:
+            ptr, dev = _ptr(levels)
+            if _nbytes(levels) < len(r) * self.graph.pred_size():
+                raise ValueError("levels buffer smaller than len(roots) * pred_size bytes")
+            check(lib().g500_msbfs_run(self.h, r.ctypes.data, len(r), ptr, int(dev), C.byref(st)))
+        return st
+
+    def levels(self, roots) -> np.ndarray:
+        """Run and return a (len(roots), pred_size) uint8 host array."""
+        out = np.empty((len(roots), self.graph.pred_size()), np.uint8)
+        self.run(roots, out)
+        return out
+
+    def root_stats(self, n: int) -> tuple[np.ndarray, np.ndarray]:
+        reached, nedge = np.zeros(n, np.int64), np.zeros(n, np.int64)
+        check(lib().g500_msbfs_root_stats(self.h, reached.ctypes.data, nedge.ctypes.data))
+        return reached, nedge
+
+    def autotune(self, roots, reps: int = 2) -> dict:
+        r = np.ascontiguousarray(roots, dtype=np.int64)
+        out = MsTune()
+        check(lib().g500_msbfs_autotune(self.h, r.ctypes.data, len(r), reps, C.byref(out)))
+        return {f[0]: getattr(out, f[0]) for f in MsTune._fields_}
+
+    def close(self) -> None:
+        if self.h is not None:
+            check(lib().g500_msbfs_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------

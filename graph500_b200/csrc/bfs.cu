@@ -31,6 +31,7 @@
 // nq > num_global_verts / alpha; BU -> TD (and stop growing) when
 // unvisited < num_global_verts / beta.
 #include "g500_internal.cuh"
+#include "device_common.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -42,7 +43,6 @@ constexpr int BFS_MIN_BLOCKS = 4;        // co-resident blocks per SM (64 regist
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
 constexpr int BU_WORDS = 8;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
 constexpr int BU_SERIAL = 6;              // row entries a lane checks alone before the warp helps
-constexpr unsigned long long SPIN_LIMIT = 1ull << 25;  // ~ seconds of __nanosleep(64)
 
 struct RunParams {
   const uint64_t* __restrict__ off;
@@ -65,120 +65,11 @@ struct RunParams {
 
 constexpr uint32_t FIRST_CHUNK = 0x80000000u;
 
-__device__ __forceinline__ unsigned long long globaltimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(FULL_MASK, x, o);
-    if (lane >= o) x += y;
-  }
-  return x;
-}
-
-__device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
-#pragma unroll
-  for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(FULL_MASK, x, o);
-  return x;
-}
-
-// last lane whose exclusive prefix is <= k (prefixes are non-decreasing over lanes)
-__device__ __forceinline__ int owner_lane(uint32_t excl, uint32_t k) {
-  int o = 0;
-#pragma unroll
-  for (int step = 16; step; step >>= 1) {
-    const uint32_t ex = __shfl_sync(FULL_MASK, excl, o + step);
-    if (ex <= k) o += step;
-  }
-  return o;
-}
-
 __device__ __forceinline__ uint32_t chunks_of(uint64_t deg) { return (uint32_t)((deg + TD_CHUNK - 1) / TD_CHUNK); }
 
 __device__ __forceinline__ void flush_counter(unsigned long long* c, unsigned long long v) {
   v = warp_sum(v);
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(c, v);
-}
-
-__device__ __forceinline__ int64_t gwarp_id() { return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
-__device__ __forceinline__ int64_t gwarp_count() { return ((int64_t)gridDim.x * blockDim.x) >> 5; }
-
-// position of the r-th (0-based) set bit of m (m has more than r set bits)
-__device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t r) {
-  uint32_t pos = 0;
-#pragma unroll
-  for (int w = 16; w; w >>= 1) {
-    const uint32_t lo = __popc(m & ((1u << w) - 1u));
-    if (r >= lo) {
-      r -= lo;
-      m >>= w;
-      pos += w;
-    } else {
-      m &= (1u << w) - 1u;
-    }
-  }
-  return pos;
-}
-
-// Add a warp's value to the block accumulator of counter i (flushed to the
-// level's global slot once per block at the next grid barrier).
-__device__ __forceinline__ void block_add(unsigned long long* sh_acc, int i, unsigned long long v) {
-  v = warp_sum(v);
-  if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh_acc[i], v);
-}
-
-// Grid-wide barrier for a cooperative launch.  The block's accumulated
-// counters are first added to flush_slot (one global atomic per counter per
-// block).  Thread 0 then arrives on a counter; the last arrival bumps the
-// generation.  Waiters spin with a bound; on timeout (or an error raised
-// elsewhere) the barrier reports failure and the caller returns.  On success
-// thread 0 copies read_slot into sh_cnt for the block's next decision.
-__device__ bool grid_sync(BfsCtl* ctl, unsigned long long* flush_slot, unsigned long long* sh_acc,
-                          const unsigned long long* read_slot, unsigned long long* sh_cnt, unsigned* sh_flag) {
-  __syncthreads();
-  if (threadIdx.x < C_NUM) {
-    const unsigned long long v = sh_acc[threadIdx.x];
-    if (flush_slot && v) atomicAdd(&flush_slot[threadIdx.x], v);
-    sh_acc[threadIdx.x] = 0;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned* gen = &ctl->bar_gen;
-    volatile unsigned* err = &ctl->err;
-    const unsigned g = *gen;
-    __threadfence();
-    bool ok = true;
-    if (atomicAdd(&ctl->bar_count, 1u) == gridDim.x - 1) {
-      ctl->bar_count = 0;
-      __threadfence();
-      atomicAdd(&ctl->bar_gen, 1u);
-    } else {
-      unsigned long long spins = 0;
-      while (*gen == g) {
-        if (*err) { ok = false; break; }
-        if (++spins > SPIN_LIMIT) {
-          atomicOr(&ctl->err, (unsigned)BFS_ERR_TIMEOUT);
-          ok = false;
-          break;
-        }
-        __nanosleep(64);
-      }
-    }
-    __threadfence();
-    if (*err) ok = false;
-    *sh_flag = ok ? 1u : 0u;
-    if (ok && read_slot) {
-      volatile const unsigned long long* vs = read_slot;
-      for (int i = 0; i < C_NUM; ++i) sh_cnt[i] = vs[i];
-    }
-  }
-  __syncthreads();
-  return *sh_flag != 0;
 }
 
 // Append the chunks of one row per lane (rows of degree < 2 and lanes with no
@@ -196,7 +87,7 @@ __device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t o
   if (lane == 31) base = atomicAdd(qcount, (unsigned long long)total);
   base = __shfl_sync(FULL_MASK, base, 31);
   if (base + total > (unsigned long long)cap) {
-    if (lane == 0) atomicOr(&ctl->err, (unsigned)BFS_ERR_QUEUE);
+    if (lane == 0) atomicOr(&ctl->bar.err, (unsigned)BFS_ERR_QUEUE);
     return;
   }
   for (uint32_t i0 = 0; i0 < total; i0 += 32) {
@@ -534,7 +425,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   const uint64_t root_b = has_edges ? p.off[root_r] : 0;
   const uint64_t root_deg = has_edges ? p.off[root_r + 1] - root_b : 0;
   const int64_t root_items = (int64_t)chunks_of(root_deg);
-  if (!grid_sync(ctl, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
+  if (!grid_sync<C_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
 
   // first_expand (bfs.hpp:477-518): the root's row becomes the first queue
   for (int64_t c = tid; c < root_items; c += nthreads) {
@@ -558,7 +449,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
     }
     return;
   }
-  if (!grid_sync(ctl, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
+  if (!grid_sync<C_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
   if (tid == 0) ctl->t_init_ns = globaltimer();
 
   int cur_vis = 0;
@@ -579,7 +470,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
     unsigned long long disc, scan = 0, edges, sect, front = 0, listed = 0, t_mid = 0, mf = 0;
     if (forward) {
       td_phase(p, items, qn, p.vis[cur_vis], found_list, cnt, sh_acc, lvl);
-      if (!grid_sync(ctl, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
+      if (!grid_sync<C_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
       if (tid == 0) t_mid = globaltimer();
       ++phase;
       disc = sh_cnt[C_DISC];
@@ -591,7 +482,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
     } else {
       uint32_t* miss = reinterpret_cast<uint32_t*>(found_list);
       bu_pass_a(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, sh_acc, lvl);
-      if (!grid_sync(ctl, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
+      if (!grid_sync<C_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
       if (tid == 0) t_mid = globaltimer();
       ++phase;
       disc = sh_cnt[C_DISC];
@@ -601,7 +492,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       if (sh_cnt[C_QITEMS] > 0) {  // some first neighbours missed
         unsigned long long* cnt_b = (NEXT_PHASE_SLOT());
         bu_pass_b(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, sh_acc, lvl);
-        if (!grid_sync(ctl, cnt_b, sh_acc, cnt_b, sh_cnt, &sh_flag)) return;
+        if (!grid_sync<C_NUM>(&ctl->bar, cnt_b, sh_acc, cnt_b, sh_cnt, &sh_flag)) return;
         ++phase;
         disc += sh_cnt[C_DISC];
         edges += sh_cnt[C_EDGES];
@@ -619,7 +510,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       break;
     }
     if (level >= MAX_LEVELS) {
-      if (tid == 0) atomicOr(&ctl->err, (unsigned)BFS_ERR_DEPTH);
+      if (tid == 0) atomicOr(&ctl->bar.err, (unsigned)BFS_ERR_DEPTH);
       break;
     }
     const int64_t unvisited = p.ngv - visited;
@@ -642,12 +533,12 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       unsigned long long* ccnt = (NEXT_PHASE_SLOT());
       if (was_forward) chunk_phase(p, found_list, (int64_t)listed, items, ccnt, sh_acc);
       else compact_phase(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], items, ccnt, sh_acc);
-      if (!grid_sync(ctl, ccnt, sh_acc, ccnt, sh_cnt, &sh_flag)) return;
+      if (!grid_sync<C_NUM>(&ctl->bar, ccnt, sh_acc, ccnt, sh_cnt, &sh_flag)) return;
       ++phase;
       qn = (int64_t)sh_cnt[C_QITEMS];
       carried = (int64_t)sh_cnt[C_SKIP];
       if (qn > p.cap) {  // append_row already flagged it; never read past the queue
-        if (tid == 0) atomicOr(&ctl->err, (unsigned)BFS_ERR_QUEUE);
+        if (tid == 0) atomicOr(&ctl->bar.err, (unsigned)BFS_ERR_QUEUE);
         return;
       }
     }
@@ -881,9 +772,9 @@ extern "C" int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_o
   G500_CUDA(cudaStreamSynchronize(s));
   b->last_root = root;
   const BfsCtl& c = *b->h_ctl;
-  if (c.err & BFS_ERR_TIMEOUT) return set_error(G500_E_TIMEOUT, "grid barrier wait gave up (bounded spin)");
-  if (c.err & BFS_ERR_QUEUE) return set_error(G500_E_RANGE, "top-down queue overflow");
-  if (c.err & BFS_ERR_DEPTH) return set_error(G500_E_RANGE, "BFS depth exceeds the 16-bit level field");
+  if (c.bar.err & BFS_ERR_TIMEOUT) return set_error(G500_E_TIMEOUT, "grid barrier wait gave up (bounded spin)");
+  if (c.bar.err & BFS_ERR_QUEUE) return set_error(G500_E_RANGE, "top-down queue overflow");
+  if (c.bar.err & BFS_ERR_DEPTH) return set_error(G500_E_RANGE, "BFS depth exceeds the 16-bit level field");
   if (stats) {
     float ms = 0;
     G500_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));

@@ -1,0 +1,125 @@
+// Device helpers shared by the persistent BFS kernels: warp scans, lane
+// selection, block-level counter accumulation and a bounded grid barrier for
+// cooperative launches.
+#pragma once
+
+#include "g500_internal.cuh"
+
+namespace g500 {
+
+constexpr unsigned long long SPIN_LIMIT = 1ull << 25;  // ~ seconds of __nanosleep(64)
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(FULL_MASK, x, o);
+    if (lane >= o) x += y;
+  }
+  return x;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(FULL_MASK, x, o);
+  return x;
+}
+
+// last lane whose exclusive prefix is <= k (prefixes are non-decreasing over lanes)
+__device__ __forceinline__ int owner_lane(uint32_t excl, uint32_t k) {
+  int o = 0;
+#pragma unroll
+  for (int step = 16; step; step >>= 1) {
+    const uint32_t ex = __shfl_sync(FULL_MASK, excl, o + step);
+    if (ex <= k) o += step;
+  }
+  return o;
+}
+
+
+
+__device__ __forceinline__ int64_t gwarp_id() { return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ int64_t gwarp_count() { return ((int64_t)gridDim.x * blockDim.x) >> 5; }
+
+// position of the r-th (0-based) set bit of m (m has more than r set bits)
+__device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t r) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (int w = 16; w; w >>= 1) {
+    const uint32_t lo = __popc(m & ((1u << w) - 1u));
+    if (r >= lo) {
+      r -= lo;
+      m >>= w;
+      pos += w;
+    } else {
+      m &= (1u << w) - 1u;
+    }
+  }
+  return pos;
+}
+
+// Add a warp's value to the block accumulator of counter i (flushed to the
+// level's global slot once per block at the next grid barrier).
+__device__ __forceinline__ void block_add(unsigned long long* sh_acc, int i, unsigned long long v) {
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh_acc[i], v);
+}
+
+// Grid-wide barrier for a cooperative launch.  The block's accumulated
+// counters are first added to flush_slot (one global atomic per counter per
+// block).  Thread 0 then arrives on a counter; the last arrival bumps the
+// generation.  Waiters spin with a bound; on timeout (or an error raised
+// elsewhere) the barrier reports failure and the caller returns.  On success
+// thread 0 copies read_slot into sh_cnt for the block's next decision.
+template <int NC>
+__device__ bool grid_sync(GridBarrier* bar, unsigned long long* flush_slot, unsigned long long* sh_acc,
+                          const unsigned long long* read_slot, unsigned long long* sh_cnt, unsigned* sh_flag) {
+  __syncthreads();
+  if (threadIdx.x < NC) {
+    const unsigned long long v = sh_acc[threadIdx.x];
+    if (flush_slot && v) atomicAdd(&flush_slot[threadIdx.x], v);
+    sh_acc[threadIdx.x] = 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = &bar->gen;
+    volatile unsigned* err = &bar->err;
+    const unsigned g = *gen;
+    __threadfence();
+    bool ok = true;
+    if (atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
+      bar->count = 0;
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      unsigned long long spins = 0;
+      while (*gen == g) {
+        if (*err) { ok = false; break; }
+        if (++spins > SPIN_LIMIT) {
+          atomicOr(&bar->err, (unsigned)GRID_ERR_TIMEOUT);
+          ok = false;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (*err) ok = false;
+    *sh_flag = ok ? 1u : 0u;
+    if (ok && read_slot) {
+      volatile const unsigned long long* vs = read_slot;
+      for (int i = 0; i < NC; ++i) sh_cnt[i] = vs[i];
+    }
+  }
+  __syncthreads();
+  return *sh_flag != 0;
+}
+
+
+}  // namespace g500

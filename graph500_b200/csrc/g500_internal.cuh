@@ -121,13 +121,21 @@ struct __align__(16) TdItem {
   uint32_t len;              // chunk length; bit 31 marks the row's first chunk
 };
 enum BfsErr { BFS_ERR_QUEUE = 1, BFS_ERR_TIMEOUT = 2, BFS_ERR_DEPTH = 4 };
+constexpr unsigned GRID_ERR_TIMEOUT = 2;  // same bit as BFS_ERR_TIMEOUT
+
+// State of a grid-wide barrier of a cooperative kernel (device memory, zeroed
+// before each launch): arrivals, generation, sticky error bits.
+struct GridBarrier {
+  unsigned count;
+  unsigned gen;
+  unsigned err;
+  unsigned pad;
+};
 
 // Control block of one run, in device memory.
 struct BfsCtl {
   unsigned long long cnt[3][C_NUM];
-  unsigned bar_count;
-  unsigned bar_gen;
-  unsigned err;
+  GridBarrier bar;
   unsigned num_levels;
   int final_vis;
   int root_has_edges;

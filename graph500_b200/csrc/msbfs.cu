@@ -1,0 +1,759 @@
+// Batched multi-source BFS: up to 128 roots per call, W = 32/64/128 roots per
+// launch as one bit-lane each in W-bit masks per vertex (visited V, frontier
+// F, next N), with a uint8 level per (vertex, lane).  Each launch is one
+// persistent cooperative kernel; every level is
+//
+//   pull   every vertex with unvisited lanes ORs its neighbours' frontier
+//          masks until all its unvisited lanes are found (bottom-up with
+//          early exit; VERTEX_REORDERING=2 puts hubs first in each row), or
+//   push   every frontier vertex ORs its mask into its neighbours' next masks
+//          (atomicOr, only the bits a neighbour still lacks),
+//
+// followed by an apply pass (new = N & ~V; V |= new; F = new; levels).  Pull
+// or push is chosen per level from edge counts: pull when the new frontier's
+// degree sum exceeds (degree sum of vertices with unvisited lanes) / alpha.
+// Levels come out per root in original-id order through a shared-memory
+// transpose; the whole launch sequence is captured once as a CUDA graph and
+// replayed for every batch.
+//
+// The levels of each lane are exactly the BFS distances from its root, the
+// same as (pred >> 48) of the plain BFS (bfs.hpp:1203, :2470).
+#include "g500_internal.cuh"
+#include "device_common.cuh"
+
+#include <algorithm>
+#include <chrono>
+
+namespace g500 {
+
+constexpr int MS_THREADS = 256;
+constexpr int MS_MIN_BLOCKS = 4;
+constexpr int MS_SERIAL = 16;      // neighbours a thread checks alone before its warp helps
+constexpr int MS_MAX_LANES = 128;
+constexpr int MS_MAX_LEVEL = 254;  // level bytes: 255 marks unreached
+enum MsCounter { M_NEW = 0, M_NF, M_MF, M_MU, M_EDGES, M_NUM = 8 };
+enum MsErr { MS_ERR_DEPTH = 4 };
+
+struct MsCtl {
+  unsigned long long cnt[3][M_NUM];
+  GridBarrier bar;
+  unsigned num_levels;
+  unsigned pull_levels;
+  unsigned long long t0_ns, t_end_ns;
+  unsigned long long level_new[MS_MAX_LEVEL + 2];
+};
+
+struct MsParams {
+  const uint64_t* __restrict__ off;
+  const uint32_t* __restrict__ col;
+  const uint32_t* __restrict__ reorder;
+  uint32_t* V;
+  uint32_t* F;
+  uint32_t* N;
+  uint8_t* L;                // [nlv][W] levels, 255 unreached
+  const int64_t* roots;      // [nroots] original ids (device)
+  const int* nroots_dev;     // number of roots of this launch (device, set with the roots)
+  int64_t nlv;
+  double alpha;
+  MsCtl* ctl;
+};
+
+template <int NW>
+struct Mask {
+  uint32_t w[NW];
+};
+
+template <int NW>
+__device__ __forceinline__ Mask<NW> load_mask(const uint32_t* p) {
+  Mask<NW> m;
+  if constexpr (NW == 4) {
+    const uint4 x = __ldcg(reinterpret_cast<const uint4*>(p));
+    m.w[0] = x.x; m.w[1] = x.y; m.w[2] = x.z; m.w[3] = x.w;
+  } else if constexpr (NW == 2) {
+    const uint2 x = __ldcg(reinterpret_cast<const uint2*>(p));
+    m.w[0] = x.x; m.w[1] = x.y;
+  } else {
+    m.w[0] = __ldcg(p);
+  }
+  return m;
+}
+
+template <int NW>
+__device__ __forceinline__ void store_mask(uint32_t* p, const Mask<NW>& m) {
+  if constexpr (NW == 4) *reinterpret_cast<uint4*>(p) = make_uint4(m.w[0], m.w[1], m.w[2], m.w[3]);
+  else if constexpr (NW == 2) *reinterpret_cast<uint2*>(p) = make_uint2(m.w[0], m.w[1]);
+  else *p = m.w[0];
+}
+
+// lanes [0, nroots) of word k
+__device__ __forceinline__ uint32_t active_word(int nroots, int k) {
+  const int lo = k * 32;
+  if (nroots >= lo + 32) return ~0u;
+  if (nroots <= lo) return 0u;
+  return (1u << (nroots - lo)) - 1u;
+}
+
+template <int NW>
+__device__ __forceinline__ bool covers(const Mask<NW>& acc, const Mask<NW>& need) {
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) ok &= (acc.w[k] & need.w[k]) == need.w[k];
+  return ok;
+}
+
+// pull: N[v] = (OR of neighbours' F) & unvisited lanes of v, for every v
+template <int NW>
+__device__ void ms_pull(const MsParams& p, const Mask<NW>& act) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = gwarp_id() * 32; base < p.nlv; base += gwarp_count() * 32) {
+    const int64_t v = base + lane;
+    Mask<NW> need, acc;
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) acc.w[k] = 0;
+    uint64_t j = 0, re = 0;
+    if (v < p.nlv) {
+      const Mask<NW> vv = load_mask<NW>(p.V + v * NW);
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        need.w[k] = act.w[k] & ~vv.w[k];
+        any |= need.w[k] != 0;
+      }
+      if (any) {
+        j = __ldg(p.off + v);
+        re = __ldg(p.off + v + 1);
+        for (int s = 0; s < MS_SERIAL && j < re; ++s, ++j) {
+          const Mask<NW> f = load_mask<NW>(p.F + (int64_t)__ldg(p.col + j) * NW);
+#pragma unroll
+          for (int k = 0; k < NW; ++k) acc.w[k] |= f.w[k];
+          if (covers<NW>(acc, need)) {
+            j = re;
+            break;
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NW; ++k) need.w[k] = 0;
+    }
+    // long rows: the warp scans them one at a time
+    unsigned rest = __ballot_sync(FULL_MASK, j < re);
+    while (rest) {
+      const int r = __ffs(rest) - 1;
+      rest &= rest - 1;
+      const uint64_t rb = __shfl_sync(FULL_MASK, j, r);
+      const uint64_t rend = __shfl_sync(FULL_MASK, re, r);
+      Mask<NW> nr, ar;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        nr.w[k] = __shfl_sync(FULL_MASK, need.w[k], r);
+        ar.w[k] = __shfl_sync(FULL_MASK, acc.w[k], r);
+      }
+      for (uint64_t p0 = rb; p0 < rend; p0 += 32) {
+        const uint64_t pp = p0 + lane;
+        Mask<NW> f;
+        if (pp < rend) f = load_mask<NW>(p.F + (int64_t)__ldg(p.col + pp) * NW);
+        else {
+#pragma unroll
+          for (int k = 0; k < NW; ++k) f.w[k] = 0;
+        }
+#pragma unroll
+        for (int k = 0; k < NW; ++k) ar.w[k] |= __reduce_or_sync(FULL_MASK, f.w[k]);
+        if (covers<NW>(ar, nr)) break;
+      }
+      if (lane == r) acc = ar;
+    }
+    if (v < p.nlv) {
+      Mask<NW> out;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) out.w[k] = acc.w[k] & need.w[k];
+      store_mask<NW>(p.N + v * NW, out);
+    }
+  }
+}
+
+// push: every frontier vertex ORs its mask into its neighbours' next masks
+template <int NW>
+__device__ void ms_push(const MsParams& p) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = gwarp_id() * 32; base < p.nlv; base += gwarp_count() * 32) {
+    const int64_t v = base + lane;
+    Mask<NW> f;
+    bool any = false;
+    uint64_t j = 0, re = 0;
+    if (v < p.nlv) {
+      f = load_mask<NW>(p.F + v * NW);
+#pragma unroll
+      for (int k = 0; k < NW; ++k) any |= f.w[k] != 0;
+      if (any) {
+        j = __ldg(p.off + v);
+        re = __ldg(p.off + v + 1);
+        for (int s = 0; s < MS_SERIAL && j < re; ++s, ++j) {
+          const int64_t w = __ldg(p.col + j);
+          const Mask<NW> vw = load_mask<NW>(p.V + w * NW);
+#pragma unroll
+          for (int k = 0; k < NW; ++k) {
+            const uint32_t add = f.w[k] & ~vw.w[k];
+            if (add) atomicOr(p.N + w * NW + k, add);
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NW; ++k) f.w[k] = 0;
+    }
+    unsigned rest = __ballot_sync(FULL_MASK, j < re);
+    while (rest) {
+      const int r = __ffs(rest) - 1;
+      rest &= rest - 1;
+      const uint64_t rb = __shfl_sync(FULL_MASK, j, r);
+      const uint64_t rend = __shfl_sync(FULL_MASK, re, r);
+      Mask<NW> fr;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) fr.w[k] = __shfl_sync(FULL_MASK, f.w[k], r);
+      for (uint64_t pp = rb + lane; pp < rend; pp += 32) {
+        const int64_t w = __ldg(p.col + pp);
+        const Mask<NW> vw = load_mask<NW>(p.V + w * NW);
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+          const uint32_t add = fr.w[k] & ~vw.w[k];
+          if (add) atomicOr(p.N + w * NW + k, add);
+        }
+      }
+    }
+  }
+}
+
+// apply: new = N & ~V; V |= new; F = new; N = 0; level bytes; counters for the
+// next direction decision.
+template <int NW>
+__device__ void ms_apply(const MsParams& p, const Mask<NW>& act, int level, unsigned long long* sh_acc) {
+  constexpr int W = 32 * NW;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  unsigned long long nnew = 0, nf = 0, mf = 0, mu = 0;
+  for (int64_t v = tid; v < p.nlv; v += nthreads) {
+    const Mask<NW> n = load_mask<NW>(p.N + v * NW);
+    const Mask<NW> vv = load_mask<NW>(p.V + v * NW);
+    Mask<NW> nw, vnew, zero;
+    bool anynew = false, done = true;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      nw.w[k] = n.w[k] & ~vv.w[k];
+      vnew.w[k] = vv.w[k] | nw.w[k];
+      zero.w[k] = 0;
+      anynew |= nw.w[k] != 0;
+      done &= (vnew.w[k] & act.w[k]) == act.w[k];
+    }
+    store_mask<NW>(p.F + v * NW, nw);
+    store_mask<NW>(p.N + v * NW, zero);
+    if (anynew) {
+      store_mask<NW>(p.V + v * NW, vnew);
+      uint8_t* row = p.L + v * W;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        uint32_t m = nw.w[k];
+        nnew += __popc(m);
+        while (m) {
+          const int b = __ffs(m) - 1;
+          m &= m - 1;
+          row[k * 32 + b] = (uint8_t)level;
+        }
+      }
+    }
+    if (anynew || !done) {
+      const uint64_t d = __ldg(p.off + v + 1) - __ldg(p.off + v);
+      if (anynew) {
+        ++nf;
+        mf += d;
+      }
+      if (!done) mu += d;
+    }
+  }
+  block_add(sh_acc, M_NEW, nnew);
+  block_add(sh_acc, M_NF, nf);
+  block_add(sh_acc, M_MF, mf);
+  block_add(sh_acc, M_MU, mu);
+}
+
+template <int NW>
+__global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsParams p) {
+  constexpr int W = 32 * NW;
+  __shared__ unsigned long long sh_cnt[M_NUM];
+  __shared__ unsigned long long sh_acc[M_NUM];
+  __shared__ unsigned sh_flag;
+  MsCtl* ctl = p.ctl;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  if (threadIdx.x < M_NUM) sh_acc[threadIdx.x] = 0;
+  const int nroots = *p.nroots_dev;
+  Mask<NW> act;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) act.w[k] = active_word(nroots, k);
+
+  if (tid == 0) ctl->t0_ns = globaltimer();
+  {
+    Mask<NW> zero;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) zero.w[k] = 0;
+    for (int64_t v = tid; v < p.nlv; v += nthreads) {
+      store_mask<NW>(p.V + v * NW, zero);
+      store_mask<NW>(p.F + v * NW, zero);
+      store_mask<NW>(p.N + v * NW, zero);
+    }
+    uint4* L16 = reinterpret_cast<uint4*>(p.L);
+    const uint4 ff = make_uint4(~0u, ~0u, ~0u, ~0u);
+    for (int64_t i = tid; i < p.nlv * (W / 16); i += nthreads) L16[i] = ff;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < 3 * M_NUM) (&ctl->cnt[0][0])[threadIdx.x] = 0;
+  if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
+
+  // roots: lane i starts at reorder[root_i] (a root outside the CSR range has
+  // no edges; its level 0 is written by the output pass)
+  unsigned long long mf0 = 0;
+  if (tid < nroots) {
+    const uint32_t r = __ldg(p.reorder + p.roots[tid]);
+    if ((int64_t)r < p.nlv) {
+      atomicOr(p.V + (int64_t)r * NW + tid / 32, 1u << (tid & 31));
+      atomicOr(p.F + (int64_t)r * NW + tid / 32, 1u << (tid & 31));
+      p.L[(int64_t)r * W + tid] = 0;
+      mf0 = __ldg(p.off + r + 1) - __ldg(p.off + r);
+    }
+  }
+  if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
+
+  bool pull = false;  // the first frontier is a handful of roots
+  unsigned phase = 0, pulls = 0;
+  int level = 1;
+  (void)mf0;
+  for (;; ++level) {
+    unsigned long long* cnt = ctl->cnt[phase % 3];
+    if (blockIdx.x == 0 && threadIdx.x < M_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
+    if (pull) ms_pull<NW>(p, act);
+    else ms_push<NW>(p);
+    pulls += pull;
+    if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
+    ms_apply<NW>(p, act, level, sh_acc);
+    if (!grid_sync<M_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
+    ++phase;
+    const unsigned long long nnew = sh_cnt[M_NEW];
+    if (tid == 0) ctl->level_new[level] = nnew;
+    if (nnew == 0) break;
+    if (level >= MS_MAX_LEVEL) {
+      if (tid == 0) atomicOr(&ctl->bar.err, (unsigned)MS_ERR_DEPTH);
+      break;
+    }
+    pull = (double)sh_cnt[M_MF] > (double)sh_cnt[M_MU] / p.alpha;
+  }
+  if (tid == 0) {
+    ctl->num_levels = (unsigned)level;
+    ctl->pull_levels = pulls;
+    ctl->t_end_ns = globaltimer();
+  }
+}
+
+// levels [nlv][W] (reordered) -> out[lane][orig] (nroots rows of nolv bytes)
+constexpr int TR_TILE = 128;
+template <int NW>
+__global__ void __launch_bounds__(256) ms_transpose_kernel(const uint8_t* __restrict__ L,
+                                                           const uint32_t* __restrict__ reorder, int64_t nlv,
+                                                           int64_t nolv, const int* nroots_dev,
+                                                           uint8_t* __restrict__ out) {
+  constexpr int W = 32 * NW;
+  __shared__ __align__(16) uint8_t tile[TR_TILE][W + 16];
+  const int nroots = *nroots_dev;
+  for (int64_t base = (int64_t)blockIdx.x * TR_TILE; base < nolv; base += (int64_t)gridDim.x * TR_TILE) {
+    // load TR_TILE rows of W bytes, 16 bytes per thread per step
+    constexpr int CHUNKS = W / 16;
+    for (int c = threadIdx.x; c < TR_TILE * CHUNKS; c += blockDim.x) {
+      const int t = c / CHUNKS, q = c % CHUNKS;
+      const int64_t u = base + t;
+      uint4 x = make_uint4(~0u, ~0u, ~0u, ~0u);
+      if (u < nolv) {
+        const uint32_t r = __ldg(reorder + u);
+        if ((int64_t)r < nlv) x = __ldg(reinterpret_cast<const uint4*>(L + (int64_t)r * W) + q);
+      }
+      *reinterpret_cast<uint4*>(&tile[t][q * 16]) = x;
+    }
+    __syncthreads();
+    // write lane rows: 4 bytes (4 consecutive vertices) per thread
+    for (int c = threadIdx.x; c < nroots * (TR_TILE / 4); c += blockDim.x) {
+      const int lane = c / (TR_TILE / 4), t4 = (c % (TR_TILE / 4)) * 4;
+      const int64_t u = base + t4;
+      if (u + 3 < nolv) {
+        const uint32_t word = (uint32_t)tile[t4][lane] | ((uint32_t)tile[t4 + 1][lane] << 8) |
+                              ((uint32_t)tile[t4 + 2][lane] << 16) | ((uint32_t)tile[t4 + 3][lane] << 24);
+        *reinterpret_cast<uint32_t*>(out + (int64_t)lane * nolv + u) = word;
+      } else {
+        for (int i = 0; i < 4 && u + i < nolv; ++i) out[(int64_t)lane * nolv + u + i] = tile[t4 + i][lane];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// every root is its own level 0 (also a root outside the CSR range)
+__global__ void ms_root_fixup_kernel(const int64_t* roots, const int* nroots_dev, int64_t nolv, uint8_t* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < *nroots_dev) out[(int64_t)i * nolv + roots[i]] = 0;
+}
+
+// per lane: reached vertices and the sum of endpoint occurrences (2 x nedge)
+template <int NW>
+__global__ void __launch_bounds__(256) ms_stats_kernel(const uint32_t* __restrict__ V,
+                                                       const uint32_t* __restrict__ endp, int64_t nlv, int nroots,
+                                                       unsigned long long* reached, unsigned long long* e2) {
+  __shared__ unsigned long long s_r[MS_MAX_LANES], s_e[MS_MAX_LANES];
+  for (int i = threadIdx.x; i < MS_MAX_LANES; i += blockDim.x) s_r[i] = s_e[i] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < nlv;
+       base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = base + lane;
+    Mask<NW> m;
+    uint32_t e = 0;
+    if (v < nlv) {
+      m = load_mask<NW>(V + v * NW);
+      e = __ldg(endp + v);
+    } else {
+#pragma unroll
+      for (int k = 0; k < NW; ++k) m.w[k] = 0;
+    }
+    for (int l = 0; l < nroots; ++l) {
+      const uint32_t bit = (m.w[l >> 5] >> (l & 31)) & 1u;
+      const unsigned rs = __reduce_add_sync(FULL_MASK, bit);
+      const unsigned es = __reduce_add_sync(FULL_MASK, bit ? e : 0u);
+      if (lane == 0 && rs) {
+        atomicAdd(&s_r[l], (unsigned long long)rs);
+        atomicAdd(&s_e[l], (unsigned long long)es);
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nroots; i += blockDim.x) {
+    if (s_r[i]) atomicAdd(&reached[i], s_r[i]);
+    if (s_e[i]) atomicAdd(&e2[i], s_e[i]);
+  }
+}
+
+}  // namespace g500
+
+using namespace g500;
+
+struct g500_msbfs {
+  g500_graph* g = nullptr;
+  cudaStream_t stream = nullptr;
+  int lane_width = 64;
+  double alpha = 15.0;
+  int use_graph = 1;
+  unsigned grid[3] = {0, 0, 0};     // co-resident blocks per lane width (NW = 1, 2, 4)
+
+  uint32_t *V = nullptr, *F = nullptr, *N = nullptr;  // [nlv][4] words (room for 128 lanes)
+  uint8_t* L = nullptr;                               // [nlv][128]
+  uint8_t* out = nullptr;                             // [128][nolv]
+  MsCtl* ctl = nullptr;                               // [4] one per batch
+  int64_t* roots_dev = nullptr;                       // [4][128]
+  int* nroots_dev = nullptr;                          // [4]
+  int64_t* staging = nullptr;                         // pinned: [4][128] roots + [4] counts
+  MsCtl* h_ctl = nullptr;                             // pinned [4]
+  unsigned long long* stats_dev = nullptr;            // [2][128]
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaGraphExec_t graphs[3][4] = {};                  // [log2(W/32)][batch]
+  int last_nroots = 0;
+  int last_batches = 0;
+};
+
+static int nw_index(int w) { return w == 32 ? 0 : (w == 64 ? 1 : 2); }
+
+static void ms_drop_graphs(g500_msbfs* m) {
+  for (auto& row : m->graphs)
+    for (auto& e : row)
+      if (e) {
+        cudaGraphExecDestroy(e);
+        e = nullptr;
+      }
+}
+
+static int ms_free(g500_msbfs* m) {
+  if (!m) return G500_OK;
+  cudaSetDevice(m->g->device);
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  ms_drop_graphs(m);
+  dev_free(m->V);
+  dev_free(m->F);
+  dev_free(m->N);
+  dev_free(m->L);
+  dev_free(m->out);
+  dev_free(m->ctl);
+  dev_free(m->roots_dev);
+  dev_free(m->nroots_dev);
+  dev_free(m->stats_dev);
+  if (m->staging) cudaFreeHost(m->staging);
+  if (m->h_ctl) cudaFreeHost(m->h_ctl);
+  if (m->ev0) cudaEventDestroy(m->ev0);
+  if (m->ev1) cudaEventDestroy(m->ev1);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+  return G500_OK;
+}
+
+template <int NW>
+static const void* ms_kernel_ptr() { return (const void*)msbfs_kernel<NW>; }
+
+// Enqueue one batch: roots upload, control reset, the persistent kernel, the
+// transpose into out + batch * W * nolv, and the root fix-up.
+static int ms_enqueue_batch(g500_msbfs* m, int b, cudaStream_t s) {
+  g500_graph* g = m->g;
+  const int W = m->lane_width;
+  const int ni = nw_index(W);
+  G500_CUDA(cudaMemcpyAsync(m->roots_dev + b * MS_MAX_LANES, m->staging + b * MS_MAX_LANES,
+                            sizeof(int64_t) * MS_MAX_LANES, cudaMemcpyHostToDevice, s));
+  G500_CUDA(cudaMemcpyAsync(m->nroots_dev + b, reinterpret_cast<int*>(m->staging + 4 * MS_MAX_LANES) + b,
+                            sizeof(int), cudaMemcpyHostToDevice, s));
+  G500_CUDA(cudaMemsetAsync(m->ctl + b, 0, sizeof(MsCtl), s));
+  MsParams p;
+  p.off = g->d_offsets;
+  p.col = g->d_cols;
+  p.reorder = g->d_reorder;
+  p.V = m->V;
+  p.F = m->F;
+  p.N = m->N;
+  p.L = m->L;
+  p.roots = m->roots_dev + b * MS_MAX_LANES;
+  p.nroots_dev = m->nroots_dev + b;
+  p.nlv = g->nlv;
+  p.alpha = m->alpha;
+  p.ctl = m->ctl + b;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(m->grid[ni]);
+  cfg.blockDim = dim3(MS_THREADS);
+  cfg.stream = s;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeCooperative;
+  attr.val.cooperative = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  if (W == 32) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<1>, p));
+  else if (W == 64) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<2>, p));
+  else G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<4>, p));
+  uint8_t* out = m->out + (int64_t)b * W * g->nolv;
+  const unsigned tg = (unsigned)std::min<int64_t>(ceil_div(g->nolv, TR_TILE), (int64_t)num_sms() * 8);
+  if (W == 32) ms_transpose_kernel<1><<<tg, 256, 0, s>>>(m->L, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
+  else if (W == 64) ms_transpose_kernel<2><<<tg, 256, 0, s>>>(m->L, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
+  else ms_transpose_kernel<4><<<tg, 256, 0, s>>>(m->L, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
+  ms_root_fixup_kernel<<<1, MS_MAX_LANES, 0, s>>>(m->roots_dev + b * MS_MAX_LANES, m->nroots_dev + b, g->nolv, out);
+  G500_CUDA(cudaGetLastError());
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_create(g500_graph* g, g500_msbfs** out) {
+  if (!g || !out) return set_error(G500_E_INVAL, "null argument");
+  G500_CUDA(cudaSetDevice(g->device));
+  g500_msbfs* m = new g500_msbfs();
+  m->g = g;
+  int st = G500_OK;
+  auto chk = [&](cudaError_t e, const char* what) {
+    if (st == G500_OK && e != cudaSuccess) st = cuda_error(e, what, __FILE__, __LINE__);
+  };
+  chk(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  const int64_t nlv = std::max<int64_t>(g->nlv, 1);
+  if (st == G500_OK) st = dev_alloc_n(&m->V, nlv * 4, "msbfs visited masks");
+  if (st == G500_OK) st = dev_alloc_n(&m->F, nlv * 4, "msbfs frontier masks");
+  if (st == G500_OK) st = dev_alloc_n(&m->N, nlv * 4, "msbfs next masks");
+  if (st == G500_OK) st = dev_alloc_n(&m->L, nlv * MS_MAX_LANES, "msbfs levels");
+  if (st == G500_OK) st = dev_alloc_n(&m->out, (int64_t)MS_MAX_LANES * g->nolv, "msbfs output levels");
+  if (st == G500_OK) st = dev_alloc_n(&m->ctl, 4, "msbfs control");
+  if (st == G500_OK) st = dev_alloc_n(&m->roots_dev, 4 * MS_MAX_LANES, "msbfs roots");
+  if (st == G500_OK) st = dev_alloc_n(&m->nroots_dev, 4, "msbfs root counts");
+  if (st == G500_OK) st = dev_alloc_n(&m->stats_dev, 2 * MS_MAX_LANES, "msbfs stats");
+  if (st == G500_OK)
+    chk(cudaHostAlloc(&m->staging, sizeof(int64_t) * (4 * MS_MAX_LANES + 4), cudaHostAllocDefault), "cudaHostAlloc");
+  if (st == G500_OK) chk(cudaHostAlloc(&m->h_ctl, sizeof(MsCtl) * 4, cudaHostAllocDefault), "cudaHostAlloc");
+  chk(cudaEventCreate(&m->ev0), "cudaEventCreate");
+  chk(cudaEventCreate(&m->ev1), "cudaEventCreate");
+  const void* kernels[3] = {ms_kernel_ptr<1>(), ms_kernel_ptr<2>(), ms_kernel_ptr<4>()};
+  for (int i = 0; i < 3 && st == G500_OK; ++i) {
+    int per_sm = 0;
+    chk(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernels[i], MS_THREADS, 0), "occupancy");
+    if (st == G500_OK && per_sm <= 0) st = set_error(G500_E_DEVICE, "multi-source kernel cannot be co-scheduled");
+    m->grid[i] = (unsigned)(num_sms() * std::max(per_sm, 1));
+  }
+  if (st != G500_OK) {
+    ms_free(m);
+    return st;
+  }
+  *out = m;
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_set_params(g500_msbfs* m, int lane_width, double alpha, int use_cuda_graph) {
+  if (!m) return set_error(G500_E_INVAL, "null handle");
+  if (lane_width != 32 && lane_width != 64 && lane_width != 128)
+    return set_error(G500_E_INVAL, "lane width %d not 32, 64 or 128", lane_width);
+  if (!(alpha > 0)) return set_error(G500_E_INVAL, "alpha must be > 0");
+  if (lane_width != m->lane_width || alpha != m->alpha) ms_drop_graphs(m);
+  m->lane_width = lane_width;
+  m->alpha = alpha;
+  m->use_graph = use_cuda_graph ? 1 : 0;
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_run(g500_msbfs* m, const int64_t* roots, int nroots, uint8_t* levels, int levels_on_device,
+                              g500_msbfs_stats* stats) {
+  if (!m || !roots) return set_error(G500_E_INVAL, "null argument");
+  g500_graph* g = m->g;
+  if (nroots < 1 || nroots > MS_MAX_LANES)
+    return set_error(G500_E_INVAL, "%d roots; 1..%d per call", nroots, MS_MAX_LANES);
+  for (int i = 0; i < nroots; ++i)
+    if (roots[i] < 0 || roots[i] >= g->nolv)
+      return set_error(G500_E_INVAL, "root %lld outside [0, %lld)", (long long)roots[i], (long long)g->nolv);
+  G500_CUDA(cudaSetDevice(g->device));
+  auto t0 = std::chrono::steady_clock::now();
+  const int W = m->lane_width;
+  const int ni = nw_index(W);
+  const int batches = (nroots + W - 1) / W;
+  int* counts = reinterpret_cast<int*>(m->staging + 4 * MS_MAX_LANES);
+  for (int b = 0; b < 4; ++b) {
+    const int n = b < batches ? std::min(W, nroots - b * W) : 0;
+    counts[b] = n;
+    for (int i = 0; i < MS_MAX_LANES; ++i) m->staging[b * MS_MAX_LANES + i] = i < n ? roots[b * W + i] : 0;
+  }
+  cudaStream_t s = m->stream;
+  G500_CUDA(cudaEventRecord(m->ev0, s));
+  for (int b = 0; b < batches; ++b) {
+    if (m->use_graph) {
+      if (!m->graphs[ni][b]) {
+        cudaGraph_t graph = nullptr;
+        G500_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        int st = ms_enqueue_batch(m, b, s);
+        cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (st != G500_OK) {
+          if (graph) cudaGraphDestroy(graph);
+          return st;
+        }
+        if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+        e = cudaGraphInstantiate(&m->graphs[ni][b], graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+          m->graphs[ni][b] = nullptr;
+          return cuda_error(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+        }
+      }
+      G500_CUDA(cudaGraphLaunch(m->graphs[ni][b], s));
+    } else {
+      G500_TRY(ms_enqueue_batch(m, b, s));
+    }
+  }
+  G500_CUDA(cudaEventRecord(m->ev1, s));
+  if (levels) {
+    G500_CUDA(cudaMemcpyAsync(levels, m->out, (size_t)nroots * g->nolv,
+                              levels_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  }
+  G500_CUDA(cudaMemcpyAsync(m->h_ctl, m->ctl, sizeof(MsCtl) * batches, cudaMemcpyDeviceToHost, s));
+  G500_CUDA(cudaStreamSynchronize(s));
+  m->last_nroots = nroots;
+  m->last_batches = batches;
+  unsigned err = 0;
+  for (int b = 0; b < batches; ++b) err |= m->h_ctl[b].bar.err;
+  if (err & GRID_ERR_TIMEOUT) return set_error(G500_E_TIMEOUT, "grid barrier wait gave up (bounded spin)");
+  if (err & MS_ERR_DEPTH) return set_error(G500_E_RANGE, "a BFS is deeper than %d levels (uint8 levels)", MS_MAX_LEVEL);
+  if (stats) {
+    float ms = 0;
+    G500_CUDA(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
+    memset(stats, 0, sizeof(*stats));
+    stats->device_ms = ms;
+    stats->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    stats->lane_width = W;
+    stats->batches = batches;
+    for (int b = 0; b < batches; ++b) {
+      stats->num_levels = std::max<int32_t>(stats->num_levels, (int32_t)m->h_ctl[b].num_levels);
+      stats->pull_levels += (int32_t)m->h_ctl[b].pull_levels;
+    }
+    stats->kernel_launches = 3 * batches;
+  }
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_root_stats(g500_msbfs* m, int64_t* reached, int64_t* nedge) {
+  if (!m) return set_error(G500_E_INVAL, "null handle");
+  if (m->last_nroots == 0) return set_error(G500_E_STATE, "no run yet");
+  if (m->last_batches != 1)
+    return set_error(G500_E_STATE, "root statistics need the last run to fit one launch (roots <= lane width)");
+  g500_graph* g = m->g;
+  G500_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = m->stream;
+  G500_CUDA(cudaMemsetAsync(m->stats_dev, 0, sizeof(unsigned long long) * 2 * MS_MAX_LANES, s));
+  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(std::max<int64_t>(g->nlv, 1), 256), num_sms() * 8);
+  const int W = m->lane_width, n = m->last_nroots;
+  unsigned long long* r = m->stats_dev;
+  unsigned long long* e = m->stats_dev + MS_MAX_LANES;
+  if (W == 32) ms_stats_kernel<1><<<grid, 256, 0, s>>>(m->V, g->d_endp, g->nlv, n, r, e);
+  else if (W == 64) ms_stats_kernel<2><<<grid, 256, 0, s>>>(m->V, g->d_endp, g->nlv, n, r, e);
+  else ms_stats_kernel<4><<<grid, 256, 0, s>>>(m->V, g->d_endp, g->nlv, n, r, e);
+  G500_CUDA(cudaGetLastError());
+  unsigned long long h[2 * MS_MAX_LANES];
+  G500_CUDA(cudaMemcpyAsync(h, m->stats_dev, sizeof(h), cudaMemcpyDeviceToHost, s));
+  G500_CUDA(cudaStreamSynchronize(s));
+  for (int i = 0; i < n; ++i) {
+    if (reached) reached[i] = (int64_t)h[i];
+    if (nedge) nedge[i] = (int64_t)(h[MS_MAX_LANES + i] / 2);
+  }
+  // a root outside the CSR range (no edges) reached only itself
+  std::vector<int64_t> rts(m->staging, m->staging + n);
+  for (int i = 0; i < n; ++i) {
+    uint32_t rr = 0;
+    G500_CUDA(cudaMemcpy(&rr, g->d_reorder + rts[(size_t)i], sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if ((int64_t)rr >= g->nlv) {
+      uint32_t ep = 0;
+      G500_CUDA(cudaMemcpy(&ep, g->d_endp + rr, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+      if (reached) reached[i] = 1;
+      if (nedge) nedge[i] = ep / 2;
+    }
+  }
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_device_levels(const g500_msbfs* m, const uint8_t** dev_levels) {
+  if (!m || !dev_levels) return set_error(G500_E_INVAL, "null argument");
+  *dev_levels = m->out;
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_autotune(g500_msbfs* m, const int64_t* roots, int nroots, int reps,
+                                   g500_msbfs_tune* out) {
+  if (!m || !roots || nroots < 1) return set_error(G500_E_INVAL, "bad argument");
+  if (reps < 1) reps = 1;
+  static const int widths[] = {32, 64, 128};
+  static const double alphas[] = {2.0, 6.0, 15.0, 50.0, 200.0};
+  const int use_graph = m->use_graph;
+  double best = 1e300;
+  int bw = 64, tried = 0;
+  double ba = 15.0;
+  for (int w : widths) {
+    for (double a : alphas) {
+      G500_TRY(g500_msbfs_set_params(m, w, a, use_graph));
+      double t = 1e300;
+      for (int k = 0; k < reps; ++k) {
+        g500_msbfs_stats st;
+        G500_TRY(g500_msbfs_run(m, roots, nroots, nullptr, 0, &st));
+        t = std::min(t, st.device_ms);
+      }
+      ++tried;
+      if (t < best) {
+        best = t;
+        bw = w;
+        ba = a;
+      }
+    }
+  }
+  G500_TRY(g500_msbfs_set_params(m, bw, ba, use_graph));
+  if (out) {
+    out->lane_width = bw;
+    out->configs_tried = tried;
+    out->alpha = ba;
+    out->best_ms = best;
+  }
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_destroy(g500_msbfs* m) { return ms_free(m); }

@@ -202,6 +202,50 @@ int g500_validate(g500_graph* g, const g500_packed_edge* edges, int64_t num_edge
                   int edges_on_device, int64_t root, const int64_t* pred, int pred_on_device,
                   int64_t* edge_visit_count, int* ok, g500_validate_report* report);
 
+/* ------------------------------------------- batched multi-source BFS */
+/* Many roots per launch: one bit-lane per root in 32/64/128-bit masks per
+ * vertex, a persistent cooperative kernel per launch, the launch sequence
+ * captured as a CUDA graph.  No counterpart in the reference, which runs one
+ * root at a time (main.cc:105-160); each root's levels equal the plain BFS's
+ * (pred >> 48) (bfs.hpp:1203, :2470). */
+typedef struct g500_msbfs_stats {
+  double device_ms;        /* CUDA-event time of all launches of the call */
+  double host_ms;          /* wall time of the call */
+  int32_t num_levels;      /* deepest launch */
+  int32_t pull_levels;     /* levels run as pull, summed over launches */
+  int32_t lane_width;
+  int32_t batches;         /* launches: ceil(roots / lane width) */
+  int32_t kernel_launches;
+  int32_t pad;
+} g500_msbfs_stats;
+
+typedef struct g500_msbfs_tune {
+  int32_t lane_width;
+  int32_t configs_tried;
+  double alpha;
+  double best_ms;
+} g500_msbfs_tune;
+
+int g500_msbfs_create(g500_graph* g, g500_msbfs** out);
+/* lane_width 32/64/128; alpha: pull when the new frontier's degree sum exceeds
+ * (degree sum of vertices with unvisited lanes) / alpha; use_cuda_graph != 0
+ * replays a captured graph per launch. */
+int g500_msbfs_set_params(g500_msbfs* m, int lane_width, double alpha, int use_cuda_graph);
+/* 1..128 roots (original ids).  levels: num_roots x pred_size bytes, root-major,
+ * original vertex ids, the BFS level or 255 if unreached; device or host
+ * memory per levels_on_device, or NULL to keep them on the device only
+ * (g500_msbfs_device_levels). */
+int g500_msbfs_run(g500_msbfs* m, const int64_t* roots, int num_roots, uint8_t* levels, int levels_on_device,
+                   g500_msbfs_stats* stats);
+/* Per root of the last run (which must have fitted one launch): vertices
+ * reached and input edges inside the reached component (validate.hpp's
+ * edge_visit_count for a valid BFS). */
+int g500_msbfs_root_stats(g500_msbfs* m, int64_t* reached, int64_t* nedge);
+int g500_msbfs_device_levels(const g500_msbfs* m, const uint8_t** dev_levels);
+/* Autotuner over lane width and alpha on sample roots (kept on the handle). */
+int g500_msbfs_autotune(g500_msbfs* m, const int64_t* roots, int num_roots, int reps, g500_msbfs_tune* out);
+int g500_msbfs_destroy(g500_msbfs* m);
+
 /* Validation that allocates nothing, for callers that cannot call cudaMalloc
  * (a host framework owning all device memory through its own arena or caching
  * allocator, or a serving loop that forbids allocation after start-up).  No
