@@ -28,7 +28,6 @@ namespace g500 {
 
 constexpr int MS_THREADS = 256;
 constexpr int MS_MIN_BLOCKS = 4;
-constexpr int MS_SERIAL = 16;      // neighbours a thread checks alone before its warp helps
 constexpr int MS_MAX_LANES = 128;
 constexpr int MS_MAX_LEVEL = 254;  // level bytes: 255 marks unreached
 enum MsCounter { M_NEW = 0, M_NF, M_MF, M_MU, M_EDGES, M_NUM = 8 };
@@ -53,6 +52,9 @@ struct MsParams {
   uint8_t* L;                // [nlv][W] levels, 255 unreached
   const int64_t* roots;      // [nroots] original ids (device)
   const int* nroots_dev;     // number of roots of this launch (device, set with the roots)
+  const uint32_t* hubs;      // rows longer than MS_HUB_DEG
+  const uint32_t* hub_chunk0;  // [nhubs] first chunk index of each hub (exclusive prefix)
+  int64_t nhubs, nhub_chunks;
   int64_t nlv;
   double alpha;
   MsCtl* ctl;
@@ -101,17 +103,34 @@ __device__ __forceinline__ bool covers(const Mask<NW>& acc, const Mask<NW>& need
   return ok;
 }
 
-// pull: N[v] = (OR of neighbours' F) & unvisited lanes of v, for every v
+constexpr int MS_WIN = 128;            // virtual edges a warp takes per window (4 per lane)
+constexpr int MS_HUB_DEG = 1024;       // rows longer than this are hub rows, split across warps
+constexpr int MS_HUB_CHUNK = 1024;     // edges of a hub row one warp takes at a time
+
+// Per-warp shared accumulators of the pull phase: 32 rows x NW words.
 template <int NW>
-__device__ void ms_pull(const MsParams& p, const Mask<NW>& act) {
+struct WarpAcc {
+  uint32_t w[32][NW];
+};
+
+// pull over non-hub rows: a warp takes 32 vertices and walks their remaining
+// edges as one concatenated list, MS_WIN edges at a time; every loaded
+// neighbour mask is ORed into its row's shared accumulator, and rows whose
+// unvisited lanes are all found leave the list.
+template <int NW>
+__device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, WarpAcc<NW>* sacc) {
   const int lane = threadIdx.x & 31;
+  WarpAcc<NW>& A = sacc[(threadIdx.x >> 5)];
   for (int64_t base = gwarp_id() * 32; base < p.nlv; base += gwarp_count() * 32) {
     const int64_t v = base + lane;
     Mask<NW> need, acc;
     bool any = false;
+    uint64_t cur = 0, re = 0;
 #pragma unroll
-    for (int k = 0; k < NW; ++k) acc.w[k] = 0;
-    uint64_t j = 0, re = 0;
+    for (int k = 0; k < NW; ++k) {
+      acc.w[k] = 0;
+      need.w[k] = 0;
+    }
     if (v < p.nlv) {
       const Mask<NW> vv = load_mask<NW>(p.V + v * NW);
 #pragma unroll
@@ -120,105 +139,174 @@ __device__ void ms_pull(const MsParams& p, const Mask<NW>& act) {
         any |= need.w[k] != 0;
       }
       if (any) {
-        j = __ldg(p.off + v);
+        cur = __ldg(p.off + v);
         re = __ldg(p.off + v + 1);
-        for (int s = 0; s < MS_SERIAL && j < re; ++s, ++j) {
-          const Mask<NW> f = load_mask<NW>(p.F + (int64_t)__ldg(p.col + j) * NW);
+        if (re - cur > (uint64_t)MS_HUB_DEG) cur = re;  // hub row: the hub phase scans it
+      }
+    }
 #pragma unroll
-          for (int k = 0; k < NW; ++k) acc.w[k] |= f.w[k];
-          if (covers<NW>(acc, need)) {
-            j = re;
-            break;
-          }
+    for (int k = 0; k < NW; ++k) A.w[lane][k] = 0;
+    bool live = any && cur < re;
+    for (;;) {
+      const uint32_t rem = live ? (uint32_t)((re - cur) < (uint64_t)MS_WIN ? (re - cur) : (uint64_t)MS_WIN) : 0u;
+      const uint32_t incl = warp_incl_scan(rem);
+      const uint32_t excl = incl - rem;
+      const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
+      if (total == 0) break;
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < MS_WIN / 32; ++j) {
+        const uint32_t k = j * 32 + lane;
+        const int o = owner_lane(excl, k);
+        const uint64_t co = __shfl_sync(FULL_MASK, cur, o);
+        const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
+        if (k < total) {
+          const Mask<NW> f = load_mask<NW>(p.F + (int64_t)__ldg(p.col + co + (k - exo)) * NW);
+#pragma unroll
+          for (int q = 0; q < NW; ++q)
+            if (f.w[q]) atomicOr(&A.w[o][q], f.w[q]);
         }
       }
-    } else {
+      __syncwarp();
+      // the window held virtual edges [0, MS_WIN): this row's share of them
+      const uint32_t used = excl >= (uint32_t)MS_WIN ? 0u : min(rem, (uint32_t)MS_WIN - excl);
+      if (live && used) {
+        cur += used;
 #pragma unroll
-      for (int k = 0; k < NW; ++k) need.w[k] = 0;
-    }
-    // long rows: the warp scans them one at a time
-    unsigned rest = __ballot_sync(FULL_MASK, j < re);
-    while (rest) {
-      const int r = __ffs(rest) - 1;
-      rest &= rest - 1;
-      const uint64_t rb = __shfl_sync(FULL_MASK, j, r);
-      const uint64_t rend = __shfl_sync(FULL_MASK, re, r);
-      Mask<NW> nr, ar;
-#pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        nr.w[k] = __shfl_sync(FULL_MASK, need.w[k], r);
-        ar.w[k] = __shfl_sync(FULL_MASK, acc.w[k], r);
+        for (int q = 0; q < NW; ++q) acc.w[q] = A.w[lane][q];
+        if (covers<NW>(acc, need) || cur >= re) live = false;
       }
-      for (uint64_t p0 = rb; p0 < rend; p0 += 32) {
-        const uint64_t pp = p0 + lane;
-        Mask<NW> f;
-        if (pp < rend) f = load_mask<NW>(p.F + (int64_t)__ldg(p.col + pp) * NW);
-        else {
-#pragma unroll
-          for (int k = 0; k < NW; ++k) f.w[k] = 0;
-        }
-#pragma unroll
-        for (int k = 0; k < NW; ++k) ar.w[k] |= __reduce_or_sync(FULL_MASK, f.w[k]);
-        if (covers<NW>(ar, nr)) break;
-      }
-      if (lane == r) acc = ar;
+      __syncwarp();
     }
-    if (v < p.nlv) {
+#pragma unroll
+    for (int q = 0; q < NW; ++q) acc.w[q] = A.w[lane][q];
+    if (v < p.nlv && !(any && __ldg(p.off + v + 1) - __ldg(p.off + v) > (uint64_t)MS_HUB_DEG)) {
       Mask<NW> out;
 #pragma unroll
       for (int k = 0; k < NW; ++k) out.w[k] = acc.w[k] & need.w[k];
       store_mask<NW>(p.N + v * NW, out);
     }
+    __syncwarp();
   }
 }
 
-// push: every frontier vertex ORs its mask into its neighbours' next masks
+// hub chunk c -> (hub vertex, first edge of the chunk)
+__device__ __forceinline__ void hub_chunk(const MsParams& p, int64_t c, uint32_t* h, uint64_t* b, uint64_t* e) {
+  int64_t lo = 0, hi = p.nhubs;  // last hub whose first chunk is <= c
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) >> 1;
+    if ((int64_t)__ldg(p.hub_chunk0 + mid) <= c) lo = mid;
+    else hi = mid;
+  }
+  *h = __ldg(p.hubs + lo);
+  const uint64_t rb = __ldg(p.off + *h), re = __ldg(p.off + *h + 1);
+  *b = rb + (uint64_t)(c - (int64_t)__ldg(p.hub_chunk0 + lo)) * MS_HUB_CHUNK;
+  *e = min(re, *b + (uint64_t)MS_HUB_CHUNK);
+}
+
+// pull over hub rows, one MS_HUB_CHUNK-edge chunk per warp at a time
 template <int NW>
-__device__ void ms_push(const MsParams& p) {
+__device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t c = gwarp_id(); c < p.nhub_chunks; c += gwarp_count()) {
+    uint32_t h;
+    uint64_t b, e;
+    hub_chunk(p, c, &h, &b, &e);
+    const Mask<NW> vv = load_mask<NW>(p.V + (int64_t)h * NW);
+    Mask<NW> need, acc;
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      need.w[k] = act.w[k] & ~vv.w[k];
+      any |= need.w[k] != 0;
+      acc.w[k] = 0;
+    }
+    if (!any) continue;
+    for (uint64_t j = b + lane; j < e; j += 32) {
+      const Mask<NW> f = load_mask<NW>(p.F + (int64_t)__ldg(p.col + j) * NW);
+#pragma unroll
+      for (int k = 0; k < NW; ++k) acc.w[k] |= f.w[k];
+    }
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const uint32_t x = __reduce_or_sync(FULL_MASK, acc.w[k]) & need.w[k];
+      if (lane == 0 && x) atomicOr(p.N + (int64_t)h * NW + k, x);
+    }
+  }
+}
+
+// push from non-hub frontier rows: 32 rows per warp, their edges walked as one
+// list MS_WIN at a time; every neighbour gets the lanes it still lacks.
+template <int NW>
+__device__ void ms_push_rows(const MsParams& p) {
   const int lane = threadIdx.x & 31;
   for (int64_t base = gwarp_id() * 32; base < p.nlv; base += gwarp_count() * 32) {
     const int64_t v = base + lane;
     Mask<NW> f;
     bool any = false;
-    uint64_t j = 0, re = 0;
+    uint64_t cur = 0, re = 0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) f.w[k] = 0;
     if (v < p.nlv) {
       f = load_mask<NW>(p.F + v * NW);
 #pragma unroll
       for (int k = 0; k < NW; ++k) any |= f.w[k] != 0;
       if (any) {
-        j = __ldg(p.off + v);
+        cur = __ldg(p.off + v);
         re = __ldg(p.off + v + 1);
-        for (int s = 0; s < MS_SERIAL && j < re; ++s, ++j) {
-          const int64_t w = __ldg(p.col + j);
+        if (re - cur > (uint64_t)MS_HUB_DEG) cur = re;  // hub row: the hub phase pushes it
+      }
+    }
+    for (;;) {
+      const uint32_t rem = (uint32_t)((re - cur) < (uint64_t)MS_WIN ? (re - cur) : (uint64_t)MS_WIN);
+      const uint32_t incl = warp_incl_scan(rem);
+      const uint32_t excl = incl - rem;
+      const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
+      if (total == 0) break;
+#pragma unroll
+      for (int j = 0; j < MS_WIN / 32; ++j) {
+        const uint32_t k = j * 32 + lane;
+        const int o = owner_lane(excl, k);
+        const uint64_t co = __shfl_sync(FULL_MASK, cur, o);
+        const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
+        Mask<NW> fo;
+#pragma unroll
+        for (int q = 0; q < NW; ++q) fo.w[q] = __shfl_sync(FULL_MASK, f.w[q], o);
+        if (k < total) {
+          const int64_t w = __ldg(p.col + co + (k - exo));
           const Mask<NW> vw = load_mask<NW>(p.V + w * NW);
 #pragma unroll
-          for (int k = 0; k < NW; ++k) {
-            const uint32_t add = f.w[k] & ~vw.w[k];
-            if (add) atomicOr(p.N + w * NW + k, add);
+          for (int q = 0; q < NW; ++q) {
+            const uint32_t add = fo.w[q] & ~vw.w[q];
+            if (add) atomicOr(p.N + w * NW + q, add);
           }
         }
       }
-    } else {
-#pragma unroll
-      for (int k = 0; k < NW; ++k) f.w[k] = 0;
+      cur += excl >= (uint32_t)MS_WIN ? 0u : min(rem, (uint32_t)MS_WIN - excl);
     }
-    unsigned rest = __ballot_sync(FULL_MASK, j < re);
-    while (rest) {
-      const int r = __ffs(rest) - 1;
-      rest &= rest - 1;
-      const uint64_t rb = __shfl_sync(FULL_MASK, j, r);
-      const uint64_t rend = __shfl_sync(FULL_MASK, re, r);
-      Mask<NW> fr;
+  }
+}
+
+// push from hub frontier rows, one chunk per warp at a time
+template <int NW>
+__device__ void ms_push_hubs(const MsParams& p) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t c = gwarp_id(); c < p.nhub_chunks; c += gwarp_count()) {
+    uint32_t h;
+    uint64_t b, e;
+    hub_chunk(p, c, &h, &b, &e);
+    const Mask<NW> f = load_mask<NW>(p.F + (int64_t)h * NW);
+    bool any = false;
 #pragma unroll
-      for (int k = 0; k < NW; ++k) fr.w[k] = __shfl_sync(FULL_MASK, f.w[k], r);
-      for (uint64_t pp = rb + lane; pp < rend; pp += 32) {
-        const int64_t w = __ldg(p.col + pp);
-        const Mask<NW> vw = load_mask<NW>(p.V + w * NW);
+    for (int k = 0; k < NW; ++k) any |= f.w[k] != 0;
+    if (!any) continue;
+    for (uint64_t j = b + lane; j < e; j += 32) {
+      const int64_t w = __ldg(p.col + j);
+      const Mask<NW> vw = load_mask<NW>(p.V + w * NW);
 #pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          const uint32_t add = fr.w[k] & ~vw.w[k];
-          if (add) atomicOr(p.N + w * NW + k, add);
-        }
+      for (int k = 0; k < NW; ++k) {
+        const uint32_t add = f.w[k] & ~vw.w[k];
+        if (add) atomicOr(p.N + w * NW + k, add);
       }
     }
   }
@@ -282,6 +370,7 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
   __shared__ unsigned long long sh_cnt[M_NUM];
   __shared__ unsigned long long sh_acc[M_NUM];
   __shared__ unsigned sh_flag;
+  __shared__ WarpAcc<NW> sacc[MS_THREADS / 32];
   MsCtl* ctl = p.ctl;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
@@ -329,8 +418,13 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
   for (;; ++level) {
     unsigned long long* cnt = ctl->cnt[phase % 3];
     if (blockIdx.x == 0 && threadIdx.x < M_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
-    if (pull) ms_pull<NW>(p, act);
-    else ms_push<NW>(p);
+    if (pull) {
+      ms_pull_rows<NW>(p, act, sacc);
+      ms_pull_hubs<NW>(p, act);
+    } else {
+      ms_push_rows<NW>(p);
+      ms_push_hubs<NW>(p);
+    }
     pulls += pull;
     if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
     ms_apply<NW>(p, act, level, sh_acc);
@@ -436,6 +530,26 @@ __global__ void __launch_bounds__(256) ms_stats_kernel(const uint32_t* __restric
   }
 }
 
+// hub list: vertices whose rows exceed MS_HUB_DEG, with their chunk counts
+__global__ void hub_flag_kernel(const uint64_t* __restrict__ off, int64_t nlv, uint32_t* flags) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nlv; r += (int64_t)gridDim.x * blockDim.x)
+    flags[r] = (off[r + 1] - off[r]) > (uint64_t)MS_HUB_DEG ? 1u : 0u;
+}
+
+__global__ void hub_compact_kernel(const uint64_t* __restrict__ off, int64_t nlv, const uint32_t* __restrict__ flags,
+                                   const uint64_t* __restrict__ pos, uint32_t* hubs, uint32_t* chunks) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nlv; r += (int64_t)gridDim.x * blockDim.x)
+    if (flags[r]) {
+      hubs[pos[r]] = (uint32_t)r;
+      chunks[pos[r]] = (uint32_t)((off[r + 1] - off[r] + MS_HUB_CHUNK - 1) / MS_HUB_CHUNK);
+    }
+}
+
+__global__ void u64_to_u32_kernel(const uint64_t* __restrict__ in, int64_t n, uint32_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)in[i];
+}
+
 }  // namespace g500
 
 using namespace g500;
@@ -459,6 +573,9 @@ struct g500_msbfs {
   unsigned long long* stats_dev = nullptr;            // [2][128]
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaGraphExec_t graphs[3][4] = {};                  // [log2(W/32)][batch]
+  uint32_t* hubs = nullptr;                           // rows longer than MS_HUB_DEG
+  uint32_t* hub_chunk0 = nullptr;                     // first chunk index of each hub
+  int64_t nhubs = 0, nhub_chunks = 0;
   int last_nroots = 0;
   int last_batches = 0;
 };
@@ -488,6 +605,8 @@ static int ms_free(g500_msbfs* m) {
   dev_free(m->roots_dev);
   dev_free(m->nroots_dev);
   dev_free(m->stats_dev);
+  dev_free(m->hubs);
+  dev_free(m->hub_chunk0);
   if (m->staging) cudaFreeHost(m->staging);
   if (m->h_ctl) cudaFreeHost(m->h_ctl);
   if (m->ev0) cudaEventDestroy(m->ev0);
@@ -499,6 +618,58 @@ static int ms_free(g500_msbfs* m) {
 
 template <int NW>
 static const void* ms_kernel_ptr() { return (const void*)msbfs_kernel<NW>; }
+
+// Hub rows (longer than MS_HUB_DEG) and the exclusive prefix of their chunk
+// counts, so warps can share a hub's row.
+static int ms_build_hubs(g500_msbfs* m) {
+  g500_graph* g = m->g;
+  cudaStream_t s = m->stream;
+  const int64_t nlv = g->nlv;
+  if (nlv == 0) return G500_OK;
+  uint32_t* flags = nullptr;
+  uint64_t* pos = nullptr;
+  uint32_t* chunks = nullptr;
+  uint64_t* chunk0 = nullptr;
+  void* tmp = nullptr;
+  int st = dev_alloc_n(&flags, nlv, "hub flags");
+  if (st == G500_OK) st = dev_alloc_n(&pos, nlv + 1, "hub positions");
+  if (st == G500_OK) st = dev_alloc(&tmp, scan_tmp_bytes(nlv + 1), "scan scratch");
+  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(nlv, 256), (int64_t)num_sms() * 8);
+  if (st == G500_OK) {
+    hub_flag_kernel<<<grid, 256, 0, s>>>(g->d_offsets, nlv, flags);
+    st = exclusive_scan_u32(flags, pos, nlv, tmp, s);
+  }
+  uint64_t H = 0;
+  if (st == G500_OK) {
+    cudaError_t e = cudaMemcpyAsync(&H, pos + nlv, sizeof(H), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cuda_error(e, "hub count", __FILE__, __LINE__);
+  }
+  m->nhubs = (int64_t)H;
+  if (st == G500_OK) st = dev_alloc_n(&m->hubs, std::max<int64_t>((int64_t)H, 1), "hub list");
+  if (st == G500_OK) st = dev_alloc_n(&chunks, std::max<int64_t>((int64_t)H, 1), "hub chunks");
+  if (st == G500_OK) st = dev_alloc_n(&chunk0, (int64_t)H + 1, "hub chunk prefix");
+  if (st == G500_OK) st = dev_alloc_n(&m->hub_chunk0, std::max<int64_t>((int64_t)H, 1), "hub chunk prefix");
+  if (st == G500_OK && H > 0) {
+    hub_compact_kernel<<<grid, 256, 0, s>>>(g->d_offsets, nlv, flags, pos, m->hubs, chunks);
+    st = exclusive_scan_u32(chunks, chunk0, (int64_t)H, tmp, s);
+    if (st == G500_OK) {
+      u64_to_u32_kernel<<<(unsigned)std::min<int64_t>(ceil_div((int64_t)H, 256), 1024), 256, 0, s>>>(chunk0, (int64_t)H,
+                                                                                                     m->hub_chunk0);
+      uint64_t tc = 0;
+      cudaError_t e = cudaMemcpyAsync(&tc, chunk0 + H, sizeof(tc), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) st = cuda_error(e, "hub chunks", __FILE__, __LINE__);
+      m->nhub_chunks = (int64_t)tc;
+    }
+  }
+  dev_free(flags);
+  dev_free(pos);
+  dev_free(chunks);
+  dev_free(chunk0);
+  dev_free(tmp);
+  return st;
+}
 
 // Enqueue one batch: roots upload, control reset, the persistent kernel, the
 // transpose into out + batch * W * nolv, and the root fix-up.
@@ -522,6 +693,10 @@ static int ms_enqueue_batch(g500_msbfs* m, int b, cudaStream_t s) {
   p.roots = m->roots_dev + b * MS_MAX_LANES;
   p.nroots_dev = m->nroots_dev + b;
   p.nlv = g->nlv;
+  p.hubs = m->hubs;
+  p.hub_chunk0 = m->hub_chunk0;
+  p.nhubs = m->nhubs;
+  p.nhub_chunks = m->nhub_chunks;
   p.alpha = m->alpha;
   p.ctl = m->ctl + b;
   cudaLaunchConfig_t cfg = {};
@@ -571,6 +746,7 @@ extern "C" int g500_msbfs_create(g500_graph* g, g500_msbfs** out) {
   if (st == G500_OK) chk(cudaHostAlloc(&m->h_ctl, sizeof(MsCtl) * 4, cudaHostAllocDefault), "cudaHostAlloc");
   chk(cudaEventCreate(&m->ev0), "cudaEventCreate");
   chk(cudaEventCreate(&m->ev1), "cudaEventCreate");
+  if (st == G500_OK) st = ms_build_hubs(m);
   const void* kernels[3] = {ms_kernel_ptr<1>(), ms_kernel_ptr<2>(), ms_kernel_ptr<4>()};
   for (int i = 0; i < 3 && st == G500_OK; ++i) {
     int per_sm = 0;
