@@ -69,12 +69,18 @@ DIR_REFERENCE, DIR_EDGES = 0, 1
 class MsStats(C.Structure):
     _fields_ = [("device_ms", C.c_double), ("host_ms", C.c_double), ("num_levels", C.c_int32),
                 ("pull_levels", C.c_int32), ("lane_width", C.c_int32), ("batches", C.c_int32),
-                ("kernel_launches", C.c_int32), ("pad", C.c_int32)]
+                ("kernel_launches", C.c_int32), ("pad", C.c_int32), ("init_ms", C.c_double),
+                ("search_ms", C.c_double)]
 
 
 class MsTune(C.Structure):
     _fields_ = [("lane_width", C.c_int32), ("configs_tried", C.c_int32), ("alpha", C.c_double),
                 ("best_ms", C.c_double)]
+
+
+class MsLevel(C.Structure):
+    _fields_ = [("level", C.c_int32), ("pull", C.c_int32), ("discovered", C.c_int64), ("device_ms", C.c_double),
+                ("expand_ms", C.c_double)]
 
 
 class ValidateReport(C.Structure):
@@ -133,6 +139,7 @@ def lib() -> C.CDLL:
         "g500_msbfs_run": ([P, P, i32, P, i32, C.POINTER(MsStats)], i32),
         "g500_msbfs_root_stats": ([P, P, P], i32),
         "g500_msbfs_device_levels": ([P, C.POINTER(P)], i32),
+        "g500_msbfs_level_info": ([P, i32, C.POINTER(MsLevel), i32, C.POINTER(i32)], i32),
         "g500_msbfs_autotune": ([P, P, i32, i32, C.POINTER(MsTune)], i32),
         "g500_msbfs_destroy": ([P], i32),
         "g500_validate_noalloc": ([P, i64, i64, i64, i64, P, P, C.POINTER(i64), C.POINTER(i32),
@@ -444,6 +451,14 @@ class MultiSourceBFS:
         reached, nedge = np.zeros(n, np.int64), np.zeros(n, np.int64)
         check(lib().g500_msbfs_root_stats(self.h, reached.ctypes.data, nedge.ctypes.data))
         return reached, nedge
+
+    def level_info(self, batch: int = 0) -> list[dict]:
+        """Per level of launch `batch` of the last run: direction, discovered
+        (vertex, root) pairs and device milliseconds."""
+        buf = (MsLevel * 256)()
+        n = C.c_int32()
+        check(lib().g500_msbfs_level_info(self.h, batch, buf, 256, C.byref(n)))
+        return [{f[0]: getattr(buf[i], f[0]) for f in MsLevel._fields_} for i in range(min(n.value, 256))]
 
     def autotune(self, roots, reps: int = 2) -> dict:
         r = np.ascontiguousarray(roots, dtype=np.int64)

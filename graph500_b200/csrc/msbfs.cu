@@ -38,12 +38,17 @@ struct MsCtl {
   GridBarrier bar;
   unsigned num_levels;
   unsigned pull_levels;
-  unsigned long long t0_ns, t_end_ns;
+  unsigned long long t0_ns, t_init_ns, t_end_ns;
+  unsigned alive[3][4];      // lanes that found vertices in the phase (rotating like cnt)
   unsigned long long level_new[MS_MAX_LEVEL + 2];
+  unsigned long long level_t_ns[MS_MAX_LEVEL + 2];
+  unsigned long long level_mid_ns[MS_MAX_LEVEL + 2];  // end of the pull/push phase
+  unsigned char level_pull[MS_MAX_LEVEL + 2];
 };
 
 struct MsParams {
   const uint64_t* __restrict__ off;
+  const uint32_t* __restrict__ deg;  // off[v + 1] - off[v]
   const uint32_t* __restrict__ col;
   const uint32_t* __restrict__ reorder;
   uint32_t* V;
@@ -52,9 +57,8 @@ struct MsParams {
   uint8_t* L;                // [nlv][W] levels, 255 unreached
   const int64_t* roots;      // [nroots] original ids (device)
   const int* nroots_dev;     // number of roots of this launch (device, set with the roots)
-  const uint32_t* hubs;      // rows longer than MS_HUB_DEG
-  const uint32_t* hub_chunk0;  // [nhubs] first chunk index of each hub (exclusive prefix)
-  int64_t nhubs, nhub_chunks;
+  const uint2* hub_tab;      // [nhub_chunks] (hub row, chunk index within the row)
+  int64_t nhub_chunks;
   int64_t nlv;
   double alpha;
   MsCtl* ctl;
@@ -87,6 +91,26 @@ __device__ __forceinline__ void store_mask(uint32_t* p, const Mask<NW>& m) {
   else *p = m.w[0];
 }
 
+// Frontier masks gathered by the pull phase use plain loads, which may hit
+// L1: hub rows recur in many adjacency lists.  The masks are rewritten by the
+// apply pass of the same launch; the grid barrier between that pass and the
+// next level (fence and atomic arrive on one side, fence after the generation
+// is seen on the other) orders those writes before these loads.
+template <int NW>
+__device__ __forceinline__ Mask<NW> gather_mask(const uint32_t* p) {
+  Mask<NW> m;
+  if constexpr (NW == 4) {
+    const uint4 x = *reinterpret_cast<const uint4*>(p);
+    m.w[0] = x.x; m.w[1] = x.y; m.w[2] = x.z; m.w[3] = x.w;
+  } else if constexpr (NW == 2) {
+    const uint2 x = *reinterpret_cast<const uint2*>(p);
+    m.w[0] = x.x; m.w[1] = x.y;
+  } else {
+    m.w[0] = *p;
+  }
+  return m;
+}
+
 // lanes [0, nroots) of word k
 __device__ __forceinline__ uint32_t active_word(int nroots, int k) {
   const int lo = k * 32;
@@ -103,29 +127,28 @@ __device__ __forceinline__ bool covers(const Mask<NW>& acc, const Mask<NW>& need
   return ok;
 }
 
-constexpr int MS_WIN = 128;            // virtual edges a warp takes per window (4 per lane)
+constexpr int MS_WIN = 128;            // push: virtual edges a warp takes per window (4 per lane)
+constexpr int MS_GROUPS = 4;           // push: groups of 32 rows whose frontier masks load together
+constexpr int MS_SMALL_DEG = 32;       // pull: rows up to this long are walked by one thread
+constexpr int MS_UNROLL = 4;           // pull: neighbours each thread loads per step
 constexpr int MS_HUB_DEG = 1024;       // rows longer than this are hub rows, split across warps
 constexpr int MS_HUB_CHUNK = 1024;     // edges of a hub row one warp takes at a time
 
-// Per-warp shared accumulators of the pull phase: 32 rows x NW words.
-template <int NW>
-struct WarpAcc {
-  uint32_t w[32][NW];
-};
 
-// pull over non-hub rows: a warp takes 32 vertices and walks their remaining
-// edges as one concatenated list, MS_WIN edges at a time; every loaded
-// neighbour mask is ORed into its row's shared accumulator, and rows whose
-// unvisited lanes are all found leave the list.
+// pull over non-hub rows.  A row of at most MS_SMALL_DEG edges is walked by
+// its own thread, MS_UNROLL neighbours per step; a longer one by the whole
+// warp, 32 * MS_UNROLL neighbours per step (rows taken in turn).  Either stops
+// once the row's unvisited lanes are all found; under VERTEX_REORDERING=2 a
+// row lists its highest-degree neighbours first, which find most of them.
 template <int NW>
-__device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, WarpAcc<NW>* sacc) {
+__device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act) {
   const int lane = threadIdx.x & 31;
-  WarpAcc<NW>& A = sacc[(threadIdx.x >> 5)];
   for (int64_t base = gwarp_id() * 32; base < p.nlv; base += gwarp_count() * 32) {
     const int64_t v = base + lane;
     Mask<NW> need, acc;
     bool any = false;
-    uint64_t cur = 0, re = 0;
+    uint32_t deg = 0;
+    uint64_t rb = 0;
 #pragma unroll
     for (int k = 0; k < NW; ++k) {
       acc.w[k] = 0;
@@ -139,229 +162,382 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, WarpAcc<NW>
         any |= need.w[k] != 0;
       }
       if (any) {
-        cur = __ldg(p.off + v);
-        re = __ldg(p.off + v + 1);
-        if (re - cur > (uint64_t)MS_HUB_DEG) cur = re;  // hub row: the hub phase scans it
+        rb = __ldg(p.off + v);
+        deg = __ldg(p.deg + v);
       }
     }
+    if (any && deg <= (uint32_t)MS_SMALL_DEG) {
+      const uint64_t re = rb + deg;
+      for (uint64_t e = rb; e < re; e += MS_UNROLL) {
+        uint32_t nb[MS_UNROLL];
 #pragma unroll
-    for (int k = 0; k < NW; ++k) A.w[lane][k] = 0;
-    bool live = any && cur < re;
-    for (;;) {
-      const uint32_t rem = live ? (uint32_t)((re - cur) < (uint64_t)MS_WIN ? (re - cur) : (uint64_t)MS_WIN) : 0u;
-      const uint32_t incl = warp_incl_scan(rem);
-      const uint32_t excl = incl - rem;
-      const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
-      if (total == 0) break;
-      __syncwarp();
+        for (int t = 0; t < MS_UNROLL; ++t) nb[t] = e + t < re ? __ldg(p.col + e + t) : NO_VERTEX;
 #pragma unroll
-      for (int j = 0; j < MS_WIN / 32; ++j) {
-        const uint32_t k = j * 32 + lane;
-        const int o = owner_lane(excl, k);
-        const uint64_t co = __shfl_sync(FULL_MASK, cur, o);
-        const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
-        if (k < total) {
-          const Mask<NW> f = load_mask<NW>(p.F + (int64_t)__ldg(p.col + co + (k - exo)) * NW);
+        for (int t = 0; t < MS_UNROLL; ++t)
+          if (nb[t] != NO_VERTEX) {
+            const Mask<NW> f = gather_mask<NW>(p.F + (int64_t)nb[t] * NW);
 #pragma unroll
-          for (int q = 0; q < NW; ++q)
-            if (f.w[q]) atomicOr(&A.w[o][q], f.w[q]);
+            for (int q = 0; q < NW; ++q) acc.w[q] |= f.w[q];
+          }
+        if (covers<NW>(acc, need)) break;
+      }
+    }
+    unsigned rows = __ballot_sync(FULL_MASK, any && deg > (uint32_t)MS_SMALL_DEG && deg <= (uint32_t)MS_HUB_DEG);
+    while (rows) {
+      const int src = __ffs(rows) - 1;
+      rows &= rows - 1;
+      const uint64_t b = __shfl_sync(FULL_MASK, rb, src);
+      const uint64_t e = b + __shfl_sync(FULL_MASK, deg, src);
+      Mask<NW> nd, a;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        nd.w[k] = __shfl_sync(FULL_MASK, need.w[k], src);
+        a.w[k] = 0;
+      }
+      for (uint64_t j = b; j < e; j += 32 * MS_UNROLL) {
+        uint32_t nb[MS_UNROLL];
+#pragma unroll
+        for (int t = 0; t < MS_UNROLL; ++t) {
+          const uint64_t i = j + t * 32 + lane;
+          nb[t] = i < e ? __ldg(p.col + i) : NO_VERTEX;
         }
-      }
-      __syncwarp();
-      // the window held virtual edges [0, MS_WIN): this row's share of them
-      const uint32_t used = excl >= (uint32_t)MS_WIN ? 0u : min(rem, (uint32_t)MS_WIN - excl);
-      if (live && used) {
-        cur += used;
+        Mask<NW> x;
 #pragma unroll
-        for (int q = 0; q < NW; ++q) acc.w[q] = A.w[lane][q];
-        if (covers<NW>(acc, need) || cur >= re) live = false;
+        for (int k = 0; k < NW; ++k) x.w[k] = 0;
+#pragma unroll
+        for (int t = 0; t < MS_UNROLL; ++t)
+          if (nb[t] != NO_VERTEX) {
+            const Mask<NW> f = gather_mask<NW>(p.F + (int64_t)nb[t] * NW);
+#pragma unroll
+            for (int q = 0; q < NW; ++q) x.w[q] |= f.w[q];
+          }
+#pragma unroll
+        for (int k = 0; k < NW; ++k) a.w[k] |= __reduce_or_sync(FULL_MASK, x.w[k]);
+        if (covers<NW>(a, nd)) break;
       }
-      __syncwarp();
+      if (lane == src) acc = a;
     }
-#pragma unroll
-    for (int q = 0; q < NW; ++q) acc.w[q] = A.w[lane][q];
-    if (v < p.nlv && !(any && __ldg(p.off + v + 1) - __ldg(p.off + v) > (uint64_t)MS_HUB_DEG)) {
+    if (any && deg <= (uint32_t)MS_HUB_DEG) {
       Mask<NW> out;
+      bool found = false;
 #pragma unroll
-      for (int k = 0; k < NW; ++k) out.w[k] = acc.w[k] & need.w[k];
-      store_mask<NW>(p.N + v * NW, out);
+      for (int k = 0; k < NW; ++k) {
+        out.w[k] = acc.w[k] & need.w[k];
+        found |= out.w[k] != 0;
+      }
+      if (found) store_mask<NW>(p.N + v * NW, out);  // N is zero outside the rows that found lanes
     }
-    __syncwarp();
   }
 }
 
-// hub chunk c -> (hub vertex, first edge of the chunk)
-__device__ __forceinline__ void hub_chunk(const MsParams& p, int64_t c, uint32_t* h, uint64_t* b, uint64_t* e) {
-  int64_t lo = 0, hi = p.nhubs;  // last hub whose first chunk is <= c
-  while (hi - lo > 1) {
-    const int64_t mid = (lo + hi) >> 1;
-    if ((int64_t)__ldg(p.hub_chunk0 + mid) <= c) lo = mid;
-    else hi = mid;
-  }
-  *h = __ldg(p.hubs + lo);
-  const uint64_t rb = __ldg(p.off + *h), re = __ldg(p.off + *h + 1);
-  *b = rb + (uint64_t)(c - (int64_t)__ldg(p.hub_chunk0 + lo)) * MS_HUB_CHUNK;
-  *e = min(re, *b + (uint64_t)MS_HUB_CHUNK);
+// Hub rows are split into MS_HUB_CHUNK-edge chunks, listed in hub_tab as
+// (row, chunk index within the row).  Warp w owns chunks w, w + nwarps, ...;
+// it reads 32 of its chunk headers at once (one per lane) and works, in turn,
+// only on the chunks whose row takes part in the level.
+__device__ __forceinline__ void hub_bounds(const MsParams& p, uint32_t h, uint32_t k, uint64_t* b, uint64_t* e) {
+  const uint64_t rb = __ldg(p.off + h);
+  const uint64_t re = rb + __ldg(p.deg + h);
+  *b = rb + (uint64_t)k * MS_HUB_CHUNK;
+  *e = *b + MS_HUB_CHUNK < re ? *b + MS_HUB_CHUNK : re;
 }
 
-// pull over hub rows, one MS_HUB_CHUNK-edge chunk per warp at a time
+// pull over hub rows: each chunk ORs its neighbours' frontier masks, stopping
+// once the row's unvisited lanes are covered, into the row's next mask
 template <int NW>
 __device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act) {
   const int lane = threadIdx.x & 31;
-  for (int64_t c = gwarp_id(); c < p.nhub_chunks; c += gwarp_count()) {
-    uint32_t h;
-    uint64_t b, e;
-    hub_chunk(p, c, &h, &b, &e);
-    const Mask<NW> vv = load_mask<NW>(p.V + (int64_t)h * NW);
-    Mask<NW> need, acc;
+  const int64_t nwarps = gwarp_count();
+  for (int64_t c0 = gwarp_id(); c0 < p.nhub_chunks; c0 += 32 * nwarps) {
+    const int64_t c = c0 + lane * nwarps;
+    uint2 hd = make_uint2(0, 0);
+    Mask<NW> need;
     bool any = false;
 #pragma unroll
-    for (int k = 0; k < NW; ++k) {
-      need.w[k] = act.w[k] & ~vv.w[k];
-      any |= need.w[k] != 0;
-      acc.w[k] = 0;
-    }
-    if (!any) continue;
-    for (uint64_t j = b + lane; j < e; j += 32) {
-      const Mask<NW> f = load_mask<NW>(p.F + (int64_t)__ldg(p.col + j) * NW);
+    for (int k = 0; k < NW; ++k) need.w[k] = 0;
+    if (c < p.nhub_chunks) {
+      hd = __ldg(p.hub_tab + c);
+      const Mask<NW> vv = load_mask<NW>(p.V + (int64_t)hd.x * NW);
 #pragma unroll
-      for (int k = 0; k < NW; ++k) acc.w[k] |= f.w[k];
-    }
-#pragma unroll
-    for (int k = 0; k < NW; ++k) {
-      const uint32_t x = __reduce_or_sync(FULL_MASK, acc.w[k]) & need.w[k];
-      if (lane == 0 && x) atomicOr(p.N + (int64_t)h * NW + k, x);
-    }
-  }
-}
-
-// push from non-hub frontier rows: 32 rows per warp, their edges walked as one
-// list MS_WIN at a time; every neighbour gets the lanes it still lacks.
-template <int NW>
-__device__ void ms_push_rows(const MsParams& p) {
-  const int lane = threadIdx.x & 31;
-  for (int64_t base = gwarp_id() * 32; base < p.nlv; base += gwarp_count() * 32) {
-    const int64_t v = base + lane;
-    Mask<NW> f;
-    bool any = false;
-    uint64_t cur = 0, re = 0;
-#pragma unroll
-    for (int k = 0; k < NW; ++k) f.w[k] = 0;
-    if (v < p.nlv) {
-      f = load_mask<NW>(p.F + v * NW);
-#pragma unroll
-      for (int k = 0; k < NW; ++k) any |= f.w[k] != 0;
-      if (any) {
-        cur = __ldg(p.off + v);
-        re = __ldg(p.off + v + 1);
-        if (re - cur > (uint64_t)MS_HUB_DEG) cur = re;  // hub row: the hub phase pushes it
+      for (int k = 0; k < NW; ++k) {
+        need.w[k] = act.w[k] & ~vv.w[k];
+        any |= need.w[k] != 0;
       }
     }
-    for (;;) {
-      const uint32_t rem = (uint32_t)((re - cur) < (uint64_t)MS_WIN ? (re - cur) : (uint64_t)MS_WIN);
-      const uint32_t incl = warp_incl_scan(rem);
-      const uint32_t excl = incl - rem;
-      const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
-      if (total == 0) break;
+    unsigned todo = __ballot_sync(FULL_MASK, any);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint32_t h = __shfl_sync(FULL_MASK, hd.x, src);
+      const uint32_t kk = __shfl_sync(FULL_MASK, hd.y, src);
+      Mask<NW> nd, a;
 #pragma unroll
-      for (int j = 0; j < MS_WIN / 32; ++j) {
-        const uint32_t k = j * 32 + lane;
-        const int o = owner_lane(excl, k);
-        const uint64_t co = __shfl_sync(FULL_MASK, cur, o);
-        const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
-        Mask<NW> fo;
+      for (int k = 0; k < NW; ++k) {
+        nd.w[k] = __shfl_sync(FULL_MASK, need.w[k], src);
+        a.w[k] = 0;
+      }
+      uint64_t b, e;
+      hub_bounds(p, h, kk, &b, &e);
+      for (uint64_t j = b; j < e; j += 32 * MS_UNROLL) {
+        uint32_t nb[MS_UNROLL];
 #pragma unroll
-        for (int q = 0; q < NW; ++q) fo.w[q] = __shfl_sync(FULL_MASK, f.w[q], o);
-        if (k < total) {
-          const int64_t w = __ldg(p.col + co + (k - exo));
-          const Mask<NW> vw = load_mask<NW>(p.V + w * NW);
-#pragma unroll
-          for (int q = 0; q < NW; ++q) {
-            const uint32_t add = fo.w[q] & ~vw.w[q];
-            if (add) atomicOr(p.N + w * NW + q, add);
-          }
+        for (int t = 0; t < MS_UNROLL; ++t) {
+          const uint64_t i = j + t * 32 + lane;
+          nb[t] = i < e ? __ldg(p.col + i) : NO_VERTEX;
         }
+        Mask<NW> x;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) x.w[k] = 0;
+#pragma unroll
+        for (int t = 0; t < MS_UNROLL; ++t)
+          if (nb[t] != NO_VERTEX) {
+            const Mask<NW> f = gather_mask<NW>(p.F + (int64_t)nb[t] * NW);
+#pragma unroll
+            for (int q = 0; q < NW; ++q) x.w[q] |= f.w[q];
+          }
+#pragma unroll
+        for (int k = 0; k < NW; ++k) a.w[k] |= __reduce_or_sync(FULL_MASK, x.w[k]);
+        if (covers<NW>(a, nd)) break;
       }
-      cur += excl >= (uint32_t)MS_WIN ? 0u : min(rem, (uint32_t)MS_WIN - excl);
+      if (lane < NW) {
+        uint32_t x = 0;
+#pragma unroll
+        for (int k = 0; k < NW; ++k)
+          if (k == lane) x = a.w[k] & nd.w[k];
+        if (x) atomicOr(p.N + (int64_t)h * NW + lane, x);
+      }
     }
   }
 }
 
-// push from hub frontier rows, one chunk per warp at a time
+// push from hub frontier rows: every neighbour of the chunk gets the lanes it
+// still lacks
 template <int NW>
 __device__ void ms_push_hubs(const MsParams& p) {
   const int lane = threadIdx.x & 31;
-  for (int64_t c = gwarp_id(); c < p.nhub_chunks; c += gwarp_count()) {
-    uint32_t h;
-    uint64_t b, e;
-    hub_chunk(p, c, &h, &b, &e);
-    const Mask<NW> f = load_mask<NW>(p.F + (int64_t)h * NW);
+  const int64_t nwarps = gwarp_count();
+  for (int64_t c0 = gwarp_id(); c0 < p.nhub_chunks; c0 += 32 * nwarps) {
+    const int64_t c = c0 + lane * nwarps;
+    uint2 hd = make_uint2(0, 0);
+    Mask<NW> f;
     bool any = false;
 #pragma unroll
-    for (int k = 0; k < NW; ++k) any |= f.w[k] != 0;
-    if (!any) continue;
-    for (uint64_t j = b + lane; j < e; j += 32) {
-      const int64_t w = __ldg(p.col + j);
-      const Mask<NW> vw = load_mask<NW>(p.V + w * NW);
+    for (int k = 0; k < NW; ++k) f.w[k] = 0;
+    if (c < p.nhub_chunks) {
+      hd = __ldg(p.hub_tab + c);
+      f = load_mask<NW>(p.F + (int64_t)hd.x * NW);
 #pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        const uint32_t add = f.w[k] & ~vw.w[k];
-        if (add) atomicOr(p.N + w * NW + k, add);
+      for (int k = 0; k < NW; ++k) any |= f.w[k] != 0;
+    }
+    unsigned todo = __ballot_sync(FULL_MASK, any);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint32_t h = __shfl_sync(FULL_MASK, hd.x, src);
+      const uint32_t kk = __shfl_sync(FULL_MASK, hd.y, src);
+      Mask<NW> fo;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) fo.w[k] = __shfl_sync(FULL_MASK, f.w[k], src);
+      uint64_t b, e;
+      hub_bounds(p, h, kk, &b, &e);
+      for (uint64_t j = b; j < e; j += 32 * MS_UNROLL) {
+        uint32_t nb[MS_UNROLL];
+#pragma unroll
+        for (int t = 0; t < MS_UNROLL; ++t) {
+          const uint64_t i = j + t * 32 + lane;
+          nb[t] = i < e ? __ldg(p.col + i) : NO_VERTEX;
+        }
+#pragma unroll
+        for (int t = 0; t < MS_UNROLL; ++t)
+          if (nb[t] != NO_VERTEX) {
+            const Mask<NW> vw = load_mask<NW>(p.V + (int64_t)nb[t] * NW);
+#pragma unroll
+            for (int q = 0; q < NW; ++q) {
+              const uint32_t add = fo.w[q] & ~vw.w[q];
+              if (add) atomicOr(p.N + (int64_t)nb[t] * NW + q, add);
+            }
+          }
       }
     }
+  }
+}
+
+// push from non-hub frontier rows: the frontier masks of MS_GROUPS groups of
+// 32 rows are loaded together; each group holding frontier rows has their
+// edges walked as one list, MS_WIN at a time; every neighbour gets the lanes
+// it still lacks.
+template <int NW>
+__device__ void ms_push_rows(const MsParams& p) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = gwarp_id() * (32 * MS_GROUPS); base < p.nlv; base += gwarp_count() * (32 * MS_GROUPS)) {
+    Mask<NW> fg[MS_GROUPS];
+#pragma unroll
+    for (int g = 0; g < MS_GROUPS; ++g) {
+      const int64_t v = base + g * 32 + lane;
+      if (v < p.nlv) fg[g] = load_mask<NW>(p.F + v * NW);
+      else
+#pragma unroll
+        for (int k = 0; k < NW; ++k) fg[g].w[k] = 0;
+    }
+#pragma unroll
+    for (int g = 0; g < MS_GROUPS; ++g) {
+      const int64_t v = base + g * 32 + lane;
+      const Mask<NW> f = fg[g];
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) any |= f.w[k] != 0;
+      if (!__any_sync(FULL_MASK, any)) continue;
+      uint64_t cur = 0, re = 0;
+      if (any) {
+        cur = __ldg(p.off + v);
+        re = cur + __ldg(p.deg + v);
+        if (re - cur > (uint64_t)MS_HUB_DEG) cur = re;  // hub row: the hub phase pushes it
+      }
+      for (;;) {
+        const uint32_t rem = (uint32_t)((re - cur) < (uint64_t)MS_WIN ? (re - cur) : (uint64_t)MS_WIN);
+        const uint32_t incl = warp_incl_scan(rem);
+        const uint32_t excl = incl - rem;
+        const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
+        if (total == 0) break;
+#pragma unroll
+        for (int j = 0; j < MS_WIN / 32; ++j) {
+          const uint32_t k = j * 32 + lane;
+          const int o = owner_lane(excl, k);
+          const uint64_t co = __shfl_sync(FULL_MASK, cur, o);
+          const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
+          Mask<NW> fo;
+#pragma unroll
+          for (int q = 0; q < NW; ++q) fo.w[q] = __shfl_sync(FULL_MASK, f.w[q], o);
+          if (k < total) {
+            const int64_t w = __ldg(p.col + co + (k - exo));
+            const Mask<NW> vw = load_mask<NW>(p.V + w * NW);
+#pragma unroll
+            for (int q = 0; q < NW; ++q) {
+              const uint32_t add = fo.w[q] & ~vw.w[q];
+              if (add) atomicOr(p.N + w * NW + q, add);
+            }
+          }
+        }
+        cur += excl >= (uint32_t)MS_WIN ? 0u : min(rem, (uint32_t)MS_WIN - excl);
+      }
+    }
+  }
+}
+
+// byte mask of the 4 lanes whose bits are set in nib (bit i -> byte i)
+__device__ __forceinline__ uint32_t nibble_bytes(uint32_t nib) {
+  return ((nib * 0x00204081u) & 0x01010101u) * 0xFFu;
+}
+
+// level bytes of a row: for each 16-lane group with new lanes, write the
+// group's 16 bytes (new lanes = level, unvisited lanes = 255, lanes visited
+// before keep their byte, read back only when the group has such lanes).
+// Groups without visited lanes are never written; the output pass reads
+// them as 255 from the visited mask.
+template <int NW>
+__device__ __forceinline__ void write_levels(uint8_t* row, const Mask<NW>& nw, const Mask<NW>& vv, uint32_t lvl4) {
+#pragma unroll
+  for (int g = 0; g < 2 * NW; ++g) {
+    const uint32_t bits = (nw.w[g >> 1] >> ((g & 1) * 16)) & 0xFFFFu;
+    if (!bits) continue;
+    const uint32_t old = (vv.w[g >> 1] >> ((g & 1) * 16)) & 0xFFFFu;
+    uint4* dst = reinterpret_cast<uint4*>(row) + g;
+    uint4 o = make_uint4(~0u, ~0u, ~0u, ~0u);
+    if (old) o = __ldcg(dst);
+    uint32_t w[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint32_t bm = nibble_bytes((bits >> (4 * i)) & 0xFu);
+      w[i] = (w[i] & ~bm) | (lvl4 & bm);
+    }
+    *dst = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
 // apply: new = N & ~V; V |= new; F = new; N = 0; level bytes; counters for the
-// next direction decision.
+// next direction decision.  MS_APPLY_U vertices per thread per step, loads
+// first; only words that change are stored.
 template <int NW>
-__device__ void ms_apply(const MsParams& p, const Mask<NW>& act, int level, unsigned long long* sh_acc) {
+__device__ void ms_apply(const MsParams& p, const Mask<NW>& act, int level, unsigned long long* sh_acc,
+                         unsigned* sh_or, unsigned* alive_out) {
   constexpr int W = 32 * NW;
+  constexpr int U = NW == 4 ? 2 : 4;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  const uint32_t lvl4 = (uint32_t)level * 0x01010101u;
   unsigned long long nnew = 0, nf = 0, mf = 0, mu = 0;
-  for (int64_t v = tid; v < p.nlv; v += nthreads) {
-    const Mask<NW> n = load_mask<NW>(p.N + v * NW);
-    const Mask<NW> vv = load_mask<NW>(p.V + v * NW);
-    Mask<NW> nw, vnew, zero;
-    bool anynew = false, done = true;
+  Mask<NW> lanes_new;
 #pragma unroll
-    for (int k = 0; k < NW; ++k) {
-      nw.w[k] = n.w[k] & ~vv.w[k];
-      vnew.w[k] = vv.w[k] | nw.w[k];
-      zero.w[k] = 0;
-      anynew |= nw.w[k] != 0;
-      done &= (vnew.w[k] & act.w[k]) == act.w[k];
+  for (int k = 0; k < NW; ++k) lanes_new.w[k] = 0;
+  for (int64_t v0 = tid; v0 < p.nlv; v0 += nthreads * U) {
+    Mask<NW> n[U], vv[U], f[U];
+    uint32_t dg[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t v = v0 + u * nthreads;
+      if (v < p.nlv) {
+        n[u] = load_mask<NW>(p.N + v * NW);
+        vv[u] = load_mask<NW>(p.V + v * NW);
+        f[u] = load_mask<NW>(p.F + v * NW);
+        dg[u] = __ldg(p.deg + v);
+      } else {
+        dg[u] = 0;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) n[u].w[k] = vv[u].w[k] = f[u].w[k] = 0;
+      }
     }
-    store_mask<NW>(p.F + v * NW, nw);
-    store_mask<NW>(p.N + v * NW, zero);
-    if (anynew) {
-      store_mask<NW>(p.V + v * NW, vnew);
-      uint8_t* row = p.L + v * W;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t v = v0 + u * nthreads;
+      Mask<NW> nw, vnew;
+      bool anyn = false, anynew = false, fchg = false, done = true;
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
-        uint32_t m = nw.w[k];
-        nnew += __popc(m);
-        while (m) {
-          const int b = __ffs(m) - 1;
-          m &= m - 1;
-          row[k * 32 + b] = (uint8_t)level;
+        nw.w[k] = n[u].w[k] & ~vv[u].w[k];
+        vnew.w[k] = vv[u].w[k] | nw.w[k];
+        anyn |= n[u].w[k] != 0;
+        anynew |= nw.w[k] != 0;
+        fchg |= f[u].w[k] != nw.w[k];
+        done &= (vnew.w[k] & act.w[k]) == act.w[k];
+      }
+      if (v >= p.nlv) continue;
+      if (anyn) {
+        Mask<NW> zero;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) zero.w[k] = 0;
+        store_mask<NW>(p.N + v * NW, zero);
+      }
+      if (fchg) store_mask<NW>(p.F + v * NW, nw);
+      if (anynew) {
+        store_mask<NW>(p.V + v * NW, vnew);
+        write_levels<NW>(p.L + v * W, nw, vv[u], lvl4);
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+          lanes_new.w[k] |= nw.w[k];
+          nnew += __popc(nw.w[k]);
         }
       }
-    }
-    if (anynew || !done) {
-      const uint64_t d = __ldg(p.off + v + 1) - __ldg(p.off + v);
       if (anynew) {
         ++nf;
-        mf += d;
+        mf += dg[u];
       }
-      if (!done) mu += d;
+      if (!done) mu += dg[u];
     }
   }
   block_add(sh_acc, M_NEW, nnew);
   block_add(sh_acc, M_NF, nf);
   block_add(sh_acc, M_MF, mf);
   block_add(sh_acc, M_MU, mu);
+  // lanes that found vertices stay alive; the others have finished their BFS
+#pragma unroll
+  for (int k = 0; k < NW; ++k) {
+    const unsigned x = __reduce_or_sync(FULL_MASK, lanes_new.w[k]);
+    if ((threadIdx.x & 31) == 0 && x) atomicOr(&sh_or[k], x);
+  }
+  __syncthreads();
+  if (threadIdx.x < NW) {
+    if (sh_or[threadIdx.x]) atomicOr(&alive_out[threadIdx.x], sh_or[threadIdx.x]);
+    sh_or[threadIdx.x] = 0;
+  }
 }
 
 template <int NW>
@@ -370,11 +546,12 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
   __shared__ unsigned long long sh_cnt[M_NUM];
   __shared__ unsigned long long sh_acc[M_NUM];
   __shared__ unsigned sh_flag;
-  __shared__ WarpAcc<NW> sacc[MS_THREADS / 32];
+  __shared__ unsigned sh_or[4];
   MsCtl* ctl = p.ctl;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
   if (threadIdx.x < M_NUM) sh_acc[threadIdx.x] = 0;
+  if (threadIdx.x < 4) sh_or[threadIdx.x] = 0;
   const int nroots = *p.nroots_dev;
   Mask<NW> act;
 #pragma unroll
@@ -390,11 +567,9 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
       store_mask<NW>(p.F + v * NW, zero);
       store_mask<NW>(p.N + v * NW, zero);
     }
-    uint4* L16 = reinterpret_cast<uint4*>(p.L);
-    const uint4 ff = make_uint4(~0u, ~0u, ~0u, ~0u);
-    for (int64_t i = tid; i < p.nlv * (W / 16); i += nthreads) L16[i] = ff;
   }
   if (blockIdx.x == 0 && threadIdx.x < 3 * M_NUM) (&ctl->cnt[0][0])[threadIdx.x] = 0;
+  if (blockIdx.x == 0 && threadIdx.x < 12) (&ctl->alive[0][0])[threadIdx.x] = 0;
   if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
 
   // roots: lane i starts at reorder[root_i] (a root outside the CSR range has
@@ -411,15 +586,18 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
   }
   if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
 
+  if (tid == 0) ctl->t_init_ns = globaltimer();
   bool pull = false;  // the first frontier is a handful of roots
   unsigned phase = 0, pulls = 0;
   int level = 1;
   (void)mf0;
   for (;; ++level) {
     unsigned long long* cnt = ctl->cnt[phase % 3];
+    unsigned* alive = ctl->alive[phase % 3];
     if (blockIdx.x == 0 && threadIdx.x < M_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
+    if (blockIdx.x == 0 && threadIdx.x < 4) ctl->alive[(phase + 1) % 3][threadIdx.x] = 0;
     if (pull) {
-      ms_pull_rows<NW>(p, act, sacc);
+      ms_pull_rows<NW>(p, act);
       ms_pull_hubs<NW>(p, act);
     } else {
       ms_push_rows<NW>(p);
@@ -427,11 +605,22 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
     }
     pulls += pull;
     if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
-    ms_apply<NW>(p, act, level, sh_acc);
+    if (tid == 0) ctl->level_mid_ns[level] = globaltimer();
+    ms_apply<NW>(p, act, level, sh_acc, sh_or, alive);
     if (!grid_sync<M_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
     ++phase;
     const unsigned long long nnew = sh_cnt[M_NEW];
-    if (tid == 0) ctl->level_new[level] = nnew;
+    if (tid == 0) {
+      ctl->level_new[level] = nnew;
+      ctl->level_t_ns[level] = globaltimer();
+      ctl->level_pull[level] = pull ? 1 : 0;
+    }
+    // a lane that found nothing this level has finished: it no longer needs anything
+    {
+      volatile const unsigned* va = alive;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) act.w[k] &= va[k];
+    }
     if (nnew == 0) break;
     if (level >= MS_MAX_LEVEL) {
       if (tid == 0) atomicOr(&ctl->bar.err, (unsigned)MS_ERR_DEPTH);
@@ -446,41 +635,64 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
   }
 }
 
-// levels [nlv][W] (reordered) -> out[lane][orig] (nroots rows of nolv bytes)
-constexpr int TR_TILE = 128;
+// levels [nlv][W] (reordered) -> out[lane][orig] (nroots rows of nolv bytes).
+// One original vertex per thread: its row's visited mask and the level bytes
+// of its visited 16-lane groups (unvisited lanes read as 255) go to a
+// shared-memory tile of W / 4 + 1 words per vertex (an odd word stride, so
+// that both the row writes and the column reads below are free of bank
+// conflicts); each warp then writes 32 consecutive vertices of one lane.
+constexpr int TR_TILE = 256;
 template <int NW>
-__global__ void __launch_bounds__(256) ms_transpose_kernel(const uint8_t* __restrict__ L,
-                                                           const uint32_t* __restrict__ reorder, int64_t nlv,
-                                                           int64_t nolv, const int* nroots_dev,
-                                                           uint8_t* __restrict__ out) {
+__global__ void __launch_bounds__(TR_TILE) ms_transpose_kernel(const uint8_t* __restrict__ L,
+                                                               const uint32_t* __restrict__ V,
+                                                               const uint32_t* __restrict__ reorder, int64_t nlv,
+                                                               int64_t nolv, const int* nroots_dev,
+                                                               uint8_t* __restrict__ out) {
   constexpr int W = 32 * NW;
-  __shared__ __align__(16) uint8_t tile[TR_TILE][W + 16];
+  constexpr int CHUNKS = W / 16;
+  constexpr int SW = W / 4 + 1;
+  __shared__ uint32_t tile[TR_TILE * SW];
   const int nroots = *nroots_dev;
+  const int lane_id = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int64_t base = (int64_t)blockIdx.x * TR_TILE; base < nolv; base += (int64_t)gridDim.x * TR_TILE) {
-    // load TR_TILE rows of W bytes, 16 bytes per thread per step
-    constexpr int CHUNKS = W / 16;
-    for (int c = threadIdx.x; c < TR_TILE * CHUNKS; c += blockDim.x) {
-      const int t = c / CHUNKS, q = c % CHUNKS;
-      const int64_t u = base + t;
-      uint4 x = make_uint4(~0u, ~0u, ~0u, ~0u);
-      if (u < nolv) {
-        const uint32_t r = __ldg(reorder + u);
-        if ((int64_t)r < nlv) x = __ldg(reinterpret_cast<const uint4*>(L + (int64_t)r * W) + q);
+    const int64_t u = base + threadIdx.x;
+    uint4 x[CHUNKS];
+#pragma unroll
+    for (int q = 0; q < CHUNKS; ++q) x[q] = make_uint4(~0u, ~0u, ~0u, ~0u);
+    if (u < nolv) {
+      const uint32_t r = __ldg(reorder + u);
+      if ((int64_t)r < nlv) {
+        uint32_t vb[NW];
+#pragma unroll
+        for (int k = 0; k < NW; ++k) vb[k] = __ldg(V + (int64_t)r * NW + k);
+#pragma unroll
+        for (int q = 0; q < CHUNKS; ++q) {
+          const uint32_t bits = (vb[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
+          if (bits) {
+            x[q] = __ldg(reinterpret_cast<const uint4*>(L + (int64_t)r * W) + q);
+            x[q].x |= ~nibble_bytes(bits & 0xFu);
+            x[q].y |= ~nibble_bytes((bits >> 4) & 0xFu);
+            x[q].z |= ~nibble_bytes((bits >> 8) & 0xFu);
+            x[q].w |= ~nibble_bytes((bits >> 12) & 0xFu);
+          }
+        }
       }
-      *reinterpret_cast<uint4*>(&tile[t][q * 16]) = x;
+    }
+    uint32_t* row = tile + threadIdx.x * SW;
+#pragma unroll
+    for (int q = 0; q < CHUNKS; ++q) {
+      row[4 * q] = x[q].x;
+      row[4 * q + 1] = x[q].y;
+      row[4 * q + 2] = x[q].z;
+      row[4 * q + 3] = x[q].w;
     }
     __syncthreads();
-    // write lane rows: 4 bytes (4 consecutive vertices) per thread
-    for (int c = threadIdx.x; c < nroots * (TR_TILE / 4); c += blockDim.x) {
-      const int lane = c / (TR_TILE / 4), t4 = (c % (TR_TILE / 4)) * 4;
-      const int64_t u = base + t4;
-      if (u + 3 < nolv) {
-        const uint32_t word = (uint32_t)tile[t4][lane] | ((uint32_t)tile[t4 + 1][lane] << 8) |
-                              ((uint32_t)tile[t4 + 2][lane] << 16) | ((uint32_t)tile[t4 + 3][lane] << 24);
-        *reinterpret_cast<uint32_t*>(out + (int64_t)lane * nolv + u) = word;
-      } else {
-        for (int i = 0; i < 4 && u + i < nolv; ++i) out[(int64_t)lane * nolv + u + i] = tile[t4 + i][lane];
-      }
+    // item = (lane, 32-vertex segment); each warp takes items in turn
+    constexpr int SEGS = TR_TILE / 32;
+    for (int item = warp; item < nroots * SEGS; item += TR_TILE / 32) {
+      const int l = item / SEGS, t = (item % SEGS) * 32 + lane_id;
+      const int64_t v = base + t;
+      if (v < nolv) out[(int64_t)l * nolv + v] = (uint8_t)(tile[t * SW + (l >> 2)] >> (8 * (l & 3)));
     }
     __syncthreads();
   }
@@ -491,6 +703,12 @@ __global__ void ms_root_fixup_kernel(const int64_t* roots, const int* nroots_dev
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < *nroots_dev) out[(int64_t)i * nolv + roots[i]] = 0;
 }
+
+__global__ void ms_degree_kernel(const uint64_t* __restrict__ off, int64_t nlv, uint32_t* __restrict__ deg) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nlv; v += (int64_t)gridDim.x * blockDim.x)
+    deg[v] = (uint32_t)(off[v + 1] - off[v]);
+}
+
 
 // per lane: reached vertices and the sum of endpoint occurrences (2 x nedge)
 template <int NW>
@@ -545,9 +763,11 @@ __global__ void hub_compact_kernel(const uint64_t* __restrict__ off, int64_t nlv
     }
 }
 
-__global__ void u64_to_u32_kernel(const uint64_t* __restrict__ in, int64_t n, uint32_t* out) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = (uint32_t)in[i];
+// chunk table: hub i's chunks [chunk0[i], chunk0[i + 1]) -> (hubs[i], k)
+__global__ void hub_tab_kernel(const uint32_t* __restrict__ hubs, const uint64_t* __restrict__ chunk0, int64_t nhubs,
+                               uint2* __restrict__ tab) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nhubs; i += (int64_t)gridDim.x * blockDim.x)
+    for (uint64_t c = chunk0[i]; c < chunk0[i + 1]; ++c) tab[c] = make_uint2(hubs[i], (uint32_t)(c - chunk0[i]));
 }
 
 }  // namespace g500
@@ -573,9 +793,9 @@ struct g500_msbfs {
   unsigned long long* stats_dev = nullptr;            // [2][128]
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaGraphExec_t graphs[3][4] = {};                  // [log2(W/32)][batch]
-  uint32_t* hubs = nullptr;                           // rows longer than MS_HUB_DEG
-  uint32_t* hub_chunk0 = nullptr;                     // first chunk index of each hub
-  int64_t nhubs = 0, nhub_chunks = 0;
+  uint32_t* deg = nullptr;                            // [nlv] row lengths
+  uint2* hub_tab = nullptr;                           // [nhub_chunks] (hub row, chunk index)
+  int64_t nhub_chunks = 0;
   int last_nroots = 0;
   int last_batches = 0;
 };
@@ -605,8 +825,8 @@ static int ms_free(g500_msbfs* m) {
   dev_free(m->roots_dev);
   dev_free(m->nroots_dev);
   dev_free(m->stats_dev);
-  dev_free(m->hubs);
-  dev_free(m->hub_chunk0);
+  dev_free(m->deg);
+  dev_free(m->hub_tab);
   if (m->staging) cudaFreeHost(m->staging);
   if (m->h_ctl) cudaFreeHost(m->h_ctl);
   if (m->ev0) cudaEventDestroy(m->ev0);
@@ -628,6 +848,7 @@ static int ms_build_hubs(g500_msbfs* m) {
   if (nlv == 0) return G500_OK;
   uint32_t* flags = nullptr;
   uint64_t* pos = nullptr;
+  uint32_t* hubs = nullptr;
   uint32_t* chunks = nullptr;
   uint64_t* chunk0 = nullptr;
   void* tmp = nullptr;
@@ -645,25 +866,30 @@ static int ms_build_hubs(g500_msbfs* m) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = cuda_error(e, "hub count", __FILE__, __LINE__);
   }
-  m->nhubs = (int64_t)H;
-  if (st == G500_OK) st = dev_alloc_n(&m->hubs, std::max<int64_t>((int64_t)H, 1), "hub list");
+  if (st == G500_OK) st = dev_alloc_n(&hubs, std::max<int64_t>((int64_t)H, 1), "hub list");
   if (st == G500_OK) st = dev_alloc_n(&chunks, std::max<int64_t>((int64_t)H, 1), "hub chunks");
   if (st == G500_OK) st = dev_alloc_n(&chunk0, (int64_t)H + 1, "hub chunk prefix");
-  if (st == G500_OK) st = dev_alloc_n(&m->hub_chunk0, std::max<int64_t>((int64_t)H, 1), "hub chunk prefix");
   if (st == G500_OK && H > 0) {
-    hub_compact_kernel<<<grid, 256, 0, s>>>(g->d_offsets, nlv, flags, pos, m->hubs, chunks);
+    hub_compact_kernel<<<grid, 256, 0, s>>>(g->d_offsets, nlv, flags, pos, hubs, chunks);
     st = exclusive_scan_u32(chunks, chunk0, (int64_t)H, tmp, s);
+    uint64_t tc = 0;
     if (st == G500_OK) {
-      u64_to_u32_kernel<<<(unsigned)std::min<int64_t>(ceil_div((int64_t)H, 256), 1024), 256, 0, s>>>(chunk0, (int64_t)H,
-                                                                                                     m->hub_chunk0);
-      uint64_t tc = 0;
       cudaError_t e = cudaMemcpyAsync(&tc, chunk0 + H, sizeof(tc), cudaMemcpyDeviceToHost, s);
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);
       if (e != cudaSuccess) st = cuda_error(e, "hub chunks", __FILE__, __LINE__);
+    }
+    if (st == G500_OK) st = dev_alloc_n(&m->hub_tab, std::max<int64_t>((int64_t)tc, 1), "hub chunk table");
+    if (st == G500_OK) {
+      const unsigned hg = (unsigned)std::min<int64_t>(ceil_div((int64_t)H, 256), 1024);
+      hub_tab_kernel<<<hg, 256, 0, s>>>(hubs, chunk0, (int64_t)H, m->hub_tab);
+      cudaError_t e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) st = cuda_error(e, "hub chunk table", __FILE__, __LINE__);
       m->nhub_chunks = (int64_t)tc;
     }
   }
   dev_free(flags);
+  dev_free(hubs);
   dev_free(pos);
   dev_free(chunks);
   dev_free(chunk0);
@@ -684,6 +910,7 @@ static int ms_enqueue_batch(g500_msbfs* m, int b, cudaStream_t s) {
   G500_CUDA(cudaMemsetAsync(m->ctl + b, 0, sizeof(MsCtl), s));
   MsParams p;
   p.off = g->d_offsets;
+  p.deg = m->deg;
   p.col = g->d_cols;
   p.reorder = g->d_reorder;
   p.V = m->V;
@@ -693,9 +920,7 @@ static int ms_enqueue_batch(g500_msbfs* m, int b, cudaStream_t s) {
   p.roots = m->roots_dev + b * MS_MAX_LANES;
   p.nroots_dev = m->nroots_dev + b;
   p.nlv = g->nlv;
-  p.hubs = m->hubs;
-  p.hub_chunk0 = m->hub_chunk0;
-  p.nhubs = m->nhubs;
+  p.hub_tab = m->hub_tab;
   p.nhub_chunks = m->nhub_chunks;
   p.alpha = m->alpha;
   p.ctl = m->ctl + b;
@@ -713,9 +938,9 @@ static int ms_enqueue_batch(g500_msbfs* m, int b, cudaStream_t s) {
   else G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<4>, p));
   uint8_t* out = m->out + (int64_t)b * W * g->nolv;
   const unsigned tg = (unsigned)std::min<int64_t>(ceil_div(g->nolv, TR_TILE), (int64_t)num_sms() * 8);
-  if (W == 32) ms_transpose_kernel<1><<<tg, 256, 0, s>>>(m->L, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
-  else if (W == 64) ms_transpose_kernel<2><<<tg, 256, 0, s>>>(m->L, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
-  else ms_transpose_kernel<4><<<tg, 256, 0, s>>>(m->L, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
+  if (W == 32) ms_transpose_kernel<1><<<tg, TR_TILE, 0, s>>>(m->L, m->V, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
+  else if (W == 64) ms_transpose_kernel<2><<<tg, TR_TILE, 0, s>>>(m->L, m->V, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
+  else ms_transpose_kernel<4><<<tg, TR_TILE, 0, s>>>(m->L, m->V, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
   ms_root_fixup_kernel<<<1, MS_MAX_LANES, 0, s>>>(m->roots_dev + b * MS_MAX_LANES, m->nroots_dev + b, g->nolv, out);
   G500_CUDA(cudaGetLastError());
   return G500_OK;
@@ -736,6 +961,12 @@ extern "C" int g500_msbfs_create(g500_graph* g, g500_msbfs** out) {
   if (st == G500_OK) st = dev_alloc_n(&m->F, nlv * 4, "msbfs frontier masks");
   if (st == G500_OK) st = dev_alloc_n(&m->N, nlv * 4, "msbfs next masks");
   if (st == G500_OK) st = dev_alloc_n(&m->L, nlv * MS_MAX_LANES, "msbfs levels");
+  if (st == G500_OK) st = dev_alloc_n(&m->deg, nlv, "msbfs row lengths");
+  if (st == G500_OK && g->nlv > 0) {
+    const unsigned dgrid = (unsigned)std::min<int64_t>(ceil_div(g->nlv, 256), (int64_t)num_sms() * 8);
+    ms_degree_kernel<<<dgrid, 256, 0, m->stream>>>(g->d_offsets, g->nlv, m->deg);
+    chk(cudaGetLastError(), "row lengths");
+  }
   if (st == G500_OK) st = dev_alloc_n(&m->out, (int64_t)MS_MAX_LANES * g->nolv, "msbfs output levels");
   if (st == G500_OK) st = dev_alloc_n(&m->ctl, 4, "msbfs control");
   if (st == G500_OK) st = dev_alloc_n(&m->roots_dev, 4 * MS_MAX_LANES, "msbfs roots");
@@ -844,6 +1075,9 @@ extern "C" int g500_msbfs_run(g500_msbfs* m, const int64_t* roots, int nroots, u
     for (int b = 0; b < batches; ++b) {
       stats->num_levels = std::max<int32_t>(stats->num_levels, (int32_t)m->h_ctl[b].num_levels);
       stats->pull_levels += (int32_t)m->h_ctl[b].pull_levels;
+      const MsCtl& c = m->h_ctl[b];
+      if (c.t_init_ns >= c.t0_ns) stats->init_ms += (double)(c.t_init_ns - c.t0_ns) * 1e-6;
+      if (c.t_end_ns >= c.t_init_ns) stats->search_ms += (double)(c.t_end_ns - c.t_init_ns) * 1e-6;
     }
     stats->kernel_launches = 3 * batches;
   }
@@ -892,6 +1126,27 @@ extern "C" int g500_msbfs_root_stats(g500_msbfs* m, int64_t* reached, int64_t* n
 extern "C" int g500_msbfs_device_levels(const g500_msbfs* m, const uint8_t** dev_levels) {
   if (!m || !dev_levels) return set_error(G500_E_INVAL, "null argument");
   *dev_levels = m->out;
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_level_info(const g500_msbfs* m, int batch, g500_msbfs_level* out, int max_levels,
+                                     int* num_levels) {
+  if (!m || !num_levels) return set_error(G500_E_INVAL, "null argument");
+  if (m->last_nroots == 0) return set_error(G500_E_STATE, "no run yet");
+  if (batch < 0 || batch >= m->last_batches)
+    return set_error(G500_E_INVAL, "launch %d outside [0, %d)", batch, m->last_batches);
+  const MsCtl& c = m->h_ctl[batch];
+  const int n = (int)std::min<unsigned>(c.num_levels, (unsigned)MS_MAX_LEVEL);
+  *num_levels = n;
+  for (int l = 1; l <= n && l <= max_levels; ++l) {
+    g500_msbfs_level& r = out[l - 1];
+    r.level = l;
+    r.pull = c.level_pull[l];
+    r.discovered = (int64_t)c.level_new[l];
+    const unsigned long long prev = l == 1 ? c.t_init_ns : c.level_t_ns[l - 1];
+    r.device_ms = c.level_t_ns[l] >= prev ? (double)(c.level_t_ns[l] - prev) * 1e-6 : 0.0;
+    r.expand_ms = c.level_mid_ns[l] >= prev ? (double)(c.level_mid_ns[l] - prev) * 1e-6 : 0.0;
+  }
   return G500_OK;
 }
 

@@ -217,6 +217,8 @@ typedef struct g500_msbfs_stats {
   int32_t batches;         /* launches: ceil(roots / lane width) */
   int32_t kernel_launches;
   int32_t pad;
+  double init_ms;          /* device global timer, summed over launches: clearing the masks, seeding */
+  double search_ms;        /* device global timer, summed over launches: the levels */
 } g500_msbfs_stats;
 
 typedef struct g500_msbfs_tune {
@@ -242,6 +244,18 @@ int g500_msbfs_run(g500_msbfs* m, const int64_t* roots, int num_roots, uint8_t* 
  * edge_visit_count for a valid BFS). */
 int g500_msbfs_root_stats(g500_msbfs* m, int64_t* reached, int64_t* nedge);
 int g500_msbfs_device_levels(const g500_msbfs* m, const uint8_t** dev_levels);
+/* One level of one launch of the last run: its direction, the (vertex, root)
+ * pairs it discovered, and its device time from the kernel's global timer. */
+typedef struct g500_msbfs_level {
+  int32_t level;
+  int32_t pull;            /* 1 = pull (unvisited lanes look at the frontier), 0 = push */
+  int64_t discovered;      /* new (vertex, lane) pairs */
+  double device_ms;        /* the whole level */
+  double expand_ms;        /* its pull or push phase (the rest is the apply pass) */
+} g500_msbfs_level;
+/* Copies up to max_levels records of launch `batch` of the last run into out;
+ * *num_levels receives the launch's level count. */
+int g500_msbfs_level_info(const g500_msbfs* m, int batch, g500_msbfs_level* out, int max_levels, int* num_levels);
 /* Autotuner over lane width and alpha on sample roots (kept on the handle). */
 int g500_msbfs_autotune(g500_msbfs* m, const int64_t* roots, int num_roots, int reps, g500_msbfs_tune* out);
 int g500_msbfs_destroy(g500_msbfs* m);
