@@ -57,8 +57,10 @@ struct MsParams {
   uint8_t* L;                // [nlv][W] levels, 255 unreached
   const int64_t* roots;      // [nroots] original ids (device)
   const int* nroots_dev;     // number of roots of this launch (device, set with the roots)
-  const uint2* hub_tab;      // [nhub_chunks] (hub row, chunk index within the row)
+  const uint2* hub_tab;      // pull: [nhub_chunks] (hub row, chunk index within the row)
   int64_t nhub_chunks;
+  const uint2* push_tab;     // push: [npush_chunks] the same for rows over MS_PUSH_HUB_DEG
+  int64_t npush_chunks;
   int64_t nlv;
   double alpha;
   MsCtl* ctl;
@@ -129,10 +131,12 @@ __device__ __forceinline__ bool covers(const Mask<NW>& acc, const Mask<NW>& need
 
 constexpr int MS_WIN = 128;            // push: virtual edges a warp takes per window (4 per lane)
 constexpr int MS_GROUPS = 4;           // push: groups of 32 rows whose frontier masks load together
-constexpr int MS_SMALL_DEG = 32;       // pull: rows up to this long are walked by one thread
+constexpr int MS_SMALL_DEG = 64;       // pull: rows up to this long are walked by one thread
 constexpr int MS_UNROLL = 4;           // pull: neighbours each thread loads per step
-constexpr int MS_HUB_DEG = 1024;       // rows longer than this are hub rows, split across warps
-constexpr int MS_HUB_CHUNK = 1024;     // edges of a hub row one warp takes at a time
+constexpr int MS_HUB_DEG = 1024;       // pull: rows longer than this are hub rows, split across warps
+constexpr int MS_HUB_CHUNK = 1024;     // pull: edges of a hub row one warp takes at a time
+constexpr int MS_PUSH_HUB_DEG = 256;   // push: the same two, smaller: a push walks every edge of its
+constexpr int MS_PUSH_CHUNK = 256;     //   frontier rows, so short chunks spread the few hub rows wider
 
 
 // pull over non-hub rows.  A row of at most MS_SMALL_DEG edges is walked by
@@ -230,15 +234,19 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act) {
   }
 }
 
-// Hub rows are split into MS_HUB_CHUNK-edge chunks, listed in hub_tab as
-// (row, chunk index within the row).  Warp w owns chunks w, w + nwarps, ...;
-// it reads 32 of its chunk headers at once (one per lane) and works, in turn,
-// only on the chunks whose row takes part in the level.
+// Hub rows are split into fixed-size chunks (MS_HUB_CHUNK edges for pull,
+// MS_PUSH_CHUNK for push), listed as (row, chunk index within the row).  Warp
+// w owns chunks w, w + nwarps, ...; it reads 32 of its chunk headers at once
+// (one per lane) and works, in turn, only on the chunks whose row takes part
+// in the level.  A pull chunk stops early once its row's lanes are found, so
+// pull chunks are long; a push chunk walks all its edges, so push chunks are
+// short and spread the hub rows of a small frontier over more warps.
+template <int CHUNK>
 __device__ __forceinline__ void hub_bounds(const MsParams& p, uint32_t h, uint32_t k, uint64_t* b, uint64_t* e) {
   const uint64_t rb = __ldg(p.off + h);
   const uint64_t re = rb + __ldg(p.deg + h);
-  *b = rb + (uint64_t)k * MS_HUB_CHUNK;
-  *e = *b + MS_HUB_CHUNK < re ? *b + MS_HUB_CHUNK : re;
+  *b = rb + (uint64_t)k * CHUNK;
+  *e = *b + CHUNK < re ? *b + CHUNK : re;
 }
 
 // pull over hub rows: each chunk ORs its neighbours' frontier masks, stopping
@@ -276,7 +284,7 @@ __device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act) {
         a.w[k] = 0;
       }
       uint64_t b, e;
-      hub_bounds(p, h, kk, &b, &e);
+      hub_bounds<MS_HUB_CHUNK>(p, h, kk, &b, &e);
       for (uint64_t j = b; j < e; j += 32 * MS_UNROLL) {
         uint32_t nb[MS_UNROLL];
 #pragma unroll
@@ -315,15 +323,15 @@ template <int NW>
 __device__ void ms_push_hubs(const MsParams& p) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = gwarp_count();
-  for (int64_t c0 = gwarp_id(); c0 < p.nhub_chunks; c0 += 32 * nwarps) {
+  for (int64_t c0 = gwarp_id(); c0 < p.npush_chunks; c0 += 32 * nwarps) {
     const int64_t c = c0 + lane * nwarps;
     uint2 hd = make_uint2(0, 0);
     Mask<NW> f;
     bool any = false;
 #pragma unroll
     for (int k = 0; k < NW; ++k) f.w[k] = 0;
-    if (c < p.nhub_chunks) {
-      hd = __ldg(p.hub_tab + c);
+    if (c < p.npush_chunks) {
+      hd = __ldg(p.push_tab + c);
       f = load_mask<NW>(p.F + (int64_t)hd.x * NW);
 #pragma unroll
       for (int k = 0; k < NW; ++k) any |= f.w[k] != 0;
@@ -338,7 +346,7 @@ __device__ void ms_push_hubs(const MsParams& p) {
 #pragma unroll
       for (int k = 0; k < NW; ++k) fo.w[k] = __shfl_sync(FULL_MASK, f.w[k], src);
       uint64_t b, e;
-      hub_bounds(p, h, kk, &b, &e);
+      hub_bounds<MS_PUSH_CHUNK>(p, h, kk, &b, &e);
       for (uint64_t j = b; j < e; j += 32 * MS_UNROLL) {
         uint32_t nb[MS_UNROLL];
 #pragma unroll
@@ -390,7 +398,7 @@ __device__ void ms_push_rows(const MsParams& p) {
       if (any) {
         cur = __ldg(p.off + v);
         re = cur + __ldg(p.deg + v);
-        if (re - cur > (uint64_t)MS_HUB_DEG) cur = re;  // hub row: the hub phase pushes it
+        if (re - cur > (uint64_t)MS_PUSH_HUB_DEG) cur = re;  // hub row: the hub phase pushes it
       }
       for (;;) {
         const uint32_t rem = (uint32_t)((re - cur) < (uint64_t)MS_WIN ? (re - cur) : (uint64_t)MS_WIN);
@@ -748,18 +756,19 @@ __global__ void __launch_bounds__(256) ms_stats_kernel(const uint32_t* __restric
   }
 }
 
-// hub list: vertices whose rows exceed MS_HUB_DEG, with their chunk counts
-__global__ void hub_flag_kernel(const uint64_t* __restrict__ off, int64_t nlv, uint32_t* flags) {
+// hub list: vertices whose rows exceed `thresh`, with their chunk counts
+__global__ void hub_flag_kernel(const uint64_t* __restrict__ off, int64_t nlv, uint64_t thresh, uint32_t* flags) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nlv; r += (int64_t)gridDim.x * blockDim.x)
-    flags[r] = (off[r + 1] - off[r]) > (uint64_t)MS_HUB_DEG ? 1u : 0u;
+    flags[r] = (off[r + 1] - off[r]) > thresh ? 1u : 0u;
 }
 
 __global__ void hub_compact_kernel(const uint64_t* __restrict__ off, int64_t nlv, const uint32_t* __restrict__ flags,
-                                   const uint64_t* __restrict__ pos, uint32_t* hubs, uint32_t* chunks) {
+                                   const uint64_t* __restrict__ pos, uint64_t chunk, uint32_t* hubs,
+                                   uint32_t* chunks) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nlv; r += (int64_t)gridDim.x * blockDim.x)
     if (flags[r]) {
       hubs[pos[r]] = (uint32_t)r;
-      chunks[pos[r]] = (uint32_t)((off[r + 1] - off[r] + MS_HUB_CHUNK - 1) / MS_HUB_CHUNK);
+      chunks[pos[r]] = (uint32_t)((off[r + 1] - off[r] + chunk - 1) / chunk);
     }
 }
 
@@ -794,8 +803,10 @@ struct g500_msbfs {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaGraphExec_t graphs[3][4] = {};                  // [log2(W/32)][batch]
   uint32_t* deg = nullptr;                            // [nlv] row lengths
-  uint2* hub_tab = nullptr;                           // [nhub_chunks] (hub row, chunk index)
+  uint2* hub_tab = nullptr;                           // pull: [nhub_chunks] (hub row, chunk index)
   int64_t nhub_chunks = 0;
+  uint2* push_tab = nullptr;                          // push: [npush_chunks]
+  int64_t npush_chunks = 0;
   int last_nroots = 0;
   int last_batches = 0;
 };
@@ -827,6 +838,7 @@ static int ms_free(g500_msbfs* m) {
   dev_free(m->stats_dev);
   dev_free(m->deg);
   dev_free(m->hub_tab);
+  dev_free(m->push_tab);
   if (m->staging) cudaFreeHost(m->staging);
   if (m->h_ctl) cudaFreeHost(m->h_ctl);
   if (m->ev0) cudaEventDestroy(m->ev0);
@@ -839,9 +851,9 @@ static int ms_free(g500_msbfs* m) {
 template <int NW>
 static const void* ms_kernel_ptr() { return (const void*)msbfs_kernel<NW>; }
 
-// Hub rows (longer than MS_HUB_DEG) and the exclusive prefix of their chunk
-// counts, so warps can share a hub's row.
-static int ms_build_hubs(g500_msbfs* m) {
+// Chunk table of the rows longer than `thresh`, `chunk` edges per chunk, so
+// that warps can share a hub's row.
+static int ms_build_hubs(g500_msbfs* m, uint64_t thresh, uint64_t chunk, uint2** tab, int64_t* ntab) {
   g500_graph* g = m->g;
   cudaStream_t s = m->stream;
   const int64_t nlv = g->nlv;
@@ -857,7 +869,7 @@ static int ms_build_hubs(g500_msbfs* m) {
   if (st == G500_OK) st = dev_alloc(&tmp, scan_tmp_bytes(nlv + 1), "scan scratch");
   const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(nlv, 256), (int64_t)num_sms() * 8);
   if (st == G500_OK) {
-    hub_flag_kernel<<<grid, 256, 0, s>>>(g->d_offsets, nlv, flags);
+    hub_flag_kernel<<<grid, 256, 0, s>>>(g->d_offsets, nlv, thresh, flags);
     st = exclusive_scan_u32(flags, pos, nlv, tmp, s);
   }
   uint64_t H = 0;
@@ -870,7 +882,7 @@ static int ms_build_hubs(g500_msbfs* m) {
   if (st == G500_OK) st = dev_alloc_n(&chunks, std::max<int64_t>((int64_t)H, 1), "hub chunks");
   if (st == G500_OK) st = dev_alloc_n(&chunk0, (int64_t)H + 1, "hub chunk prefix");
   if (st == G500_OK && H > 0) {
-    hub_compact_kernel<<<grid, 256, 0, s>>>(g->d_offsets, nlv, flags, pos, hubs, chunks);
+    hub_compact_kernel<<<grid, 256, 0, s>>>(g->d_offsets, nlv, flags, pos, chunk, hubs, chunks);
     st = exclusive_scan_u32(chunks, chunk0, (int64_t)H, tmp, s);
     uint64_t tc = 0;
     if (st == G500_OK) {
@@ -878,14 +890,14 @@ static int ms_build_hubs(g500_msbfs* m) {
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);
       if (e != cudaSuccess) st = cuda_error(e, "hub chunks", __FILE__, __LINE__);
     }
-    if (st == G500_OK) st = dev_alloc_n(&m->hub_tab, std::max<int64_t>((int64_t)tc, 1), "hub chunk table");
+    if (st == G500_OK) st = dev_alloc_n(tab, std::max<int64_t>((int64_t)tc, 1), "hub chunk table");
     if (st == G500_OK) {
       const unsigned hg = (unsigned)std::min<int64_t>(ceil_div((int64_t)H, 256), 1024);
-      hub_tab_kernel<<<hg, 256, 0, s>>>(hubs, chunk0, (int64_t)H, m->hub_tab);
+      hub_tab_kernel<<<hg, 256, 0, s>>>(hubs, chunk0, (int64_t)H, *tab);
       cudaError_t e = cudaGetLastError();
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);
       if (e != cudaSuccess) st = cuda_error(e, "hub chunk table", __FILE__, __LINE__);
-      m->nhub_chunks = (int64_t)tc;
+      *ntab = (int64_t)tc;
     }
   }
   dev_free(flags);
@@ -922,6 +934,8 @@ static int ms_enqueue_batch(g500_msbfs* m, int b, cudaStream_t s) {
   p.nlv = g->nlv;
   p.hub_tab = m->hub_tab;
   p.nhub_chunks = m->nhub_chunks;
+  p.push_tab = m->push_tab;
+  p.npush_chunks = m->npush_chunks;
   p.alpha = m->alpha;
   p.ctl = m->ctl + b;
   cudaLaunchConfig_t cfg = {};
@@ -977,7 +991,8 @@ extern "C" int g500_msbfs_create(g500_graph* g, g500_msbfs** out) {
   if (st == G500_OK) chk(cudaHostAlloc(&m->h_ctl, sizeof(MsCtl) * 4, cudaHostAllocDefault), "cudaHostAlloc");
   chk(cudaEventCreate(&m->ev0), "cudaEventCreate");
   chk(cudaEventCreate(&m->ev1), "cudaEventCreate");
-  if (st == G500_OK) st = ms_build_hubs(m);
+  if (st == G500_OK) st = ms_build_hubs(m, MS_HUB_DEG, MS_HUB_CHUNK, &m->hub_tab, &m->nhub_chunks);
+  if (st == G500_OK) st = ms_build_hubs(m, MS_PUSH_HUB_DEG, MS_PUSH_CHUNK, &m->push_tab, &m->npush_chunks);
   const void* kernels[3] = {ms_kernel_ptr<1>(), ms_kernel_ptr<2>(), ms_kernel_ptr<4>()};
   for (int i = 0; i < 3 && st == G500_OK; ++i) {
     int per_sm = 0;
