@@ -643,66 +643,75 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
   }
 }
 
+// 4x4 byte transpose: c[j] byte v = a[v] byte j
+__device__ __forceinline__ void transpose4x4(const uint32_t a[4], uint32_t c[4]) {
+  const uint32_t t0 = __byte_perm(a[0], a[1], 0x5140u), t1 = __byte_perm(a[0], a[1], 0x7362u);
+  const uint32_t t2 = __byte_perm(a[2], a[3], 0x5140u), t3 = __byte_perm(a[2], a[3], 0x7362u);
+  c[0] = __byte_perm(t0, t2, 0x5410u);
+  c[1] = __byte_perm(t0, t2, 0x7632u);
+  c[2] = __byte_perm(t1, t3, 0x5410u);
+  c[3] = __byte_perm(t1, t3, 0x7632u);
+}
+
 // levels [nlv][W] (reordered) -> out[lane][orig] (nroots rows of nolv bytes).
-// One original vertex per thread: its row's visited mask and the level bytes
-// of its visited 16-lane groups (unvisited lanes read as 255) go to a
-// shared-memory tile of W / 4 + 1 words per vertex (an odd word stride, so
-// that both the row writes and the column reads below are free of bank
-// conflicts); each warp then writes 32 consecutive vertices of one lane.
-constexpr int TR_TILE = 256;
+// Four consecutive original vertices per thread: their rows' visited masks and
+// the level bytes of their visited 16-lane groups (unvisited lanes read as
+// 255).  Each 32-bit word of a row holds 4 lanes of one vertex; a 4x4 byte
+// transpose in registers turns the 4 vertices' words into 4 words of one lane
+// x 4 vertices, so every store instruction of a warp writes 128 consecutive
+// bytes of one lane's output row (nolv is a multiple of 65536, so the
+// 4-vertex steps never straddle the end).
+constexpr int TR_BLOCK = 256;
 template <int NW>
-__global__ void __launch_bounds__(TR_TILE) ms_transpose_kernel(const uint8_t* __restrict__ L,
-                                                               const uint32_t* __restrict__ V,
-                                                               const uint32_t* __restrict__ reorder, int64_t nlv,
-                                                               int64_t nolv, const int* nroots_dev,
-                                                               uint8_t* __restrict__ out) {
+__global__ void __launch_bounds__(TR_BLOCK) ms_transpose_kernel(const uint8_t* __restrict__ L,
+                                                                const uint32_t* __restrict__ V,
+                                                                const uint32_t* __restrict__ reorder, int64_t nlv,
+                                                                int64_t nolv, const int* nroots_dev,
+                                                                uint8_t* __restrict__ out) {
   constexpr int W = 32 * NW;
   constexpr int CHUNKS = W / 16;
-  constexpr int SW = W / 4 + 1;
-  __shared__ uint32_t tile[TR_TILE * SW];
   const int nroots = *nroots_dev;
-  const int lane_id = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int64_t base = (int64_t)blockIdx.x * TR_TILE; base < nolv; base += (int64_t)gridDim.x * TR_TILE) {
-    const int64_t u = base + threadIdx.x;
-    uint4 x[CHUNKS];
+  for (int64_t u0 = ((int64_t)blockIdx.x * TR_BLOCK + threadIdx.x) * 4; u0 < nolv;
+       u0 += (int64_t)gridDim.x * TR_BLOCK * 4) {
+    const uint4 rr = __ldg(reinterpret_cast<const uint4*>(reorder + u0));
+    const uint32_t r[4] = {rr.x, rr.y, rr.z, rr.w};
+    uint32_t vb[4][NW];
 #pragma unroll
-    for (int q = 0; q < CHUNKS; ++q) x[q] = make_uint4(~0u, ~0u, ~0u, ~0u);
-    if (u < nolv) {
-      const uint32_t r = __ldg(reorder + u);
-      if ((int64_t)r < nlv) {
-        uint32_t vb[NW];
+    for (int v = 0; v < 4; ++v)
 #pragma unroll
-        for (int k = 0; k < NW; ++k) vb[k] = __ldg(V + (int64_t)r * NW + k);
+      for (int k = 0; k < NW; ++k) vb[v][k] = (int64_t)r[v] < nlv ? __ldg(V + (int64_t)r[v] * NW + k) : 0u;
+    // one 16-lane group at a time (keeps the registers, hence occupancy, low)
+#pragma unroll 1
+    for (int q = 0; q < CHUNKS; ++q) {
+      uint4 x[4];
 #pragma unroll
-        for (int q = 0; q < CHUNKS; ++q) {
-          const uint32_t bits = (vb[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
-          if (bits) {
-            x[q] = __ldg(reinterpret_cast<const uint4*>(L + (int64_t)r * W) + q);
-            x[q].x |= ~nibble_bytes(bits & 0xFu);
-            x[q].y |= ~nibble_bytes((bits >> 4) & 0xFu);
-            x[q].z |= ~nibble_bytes((bits >> 8) & 0xFu);
-            x[q].w |= ~nibble_bytes((bits >> 12) & 0xFu);
-          }
+      for (int v = 0; v < 4; ++v) {
+        uint32_t word = vb[v][0];
+#pragma unroll
+        for (int k = 1; k < NW; ++k) word = (q >> 1) == k ? vb[v][k] : word;
+        const uint32_t bits = (word >> ((q & 1) * 16)) & 0xFFFFu;
+        x[v] = make_uint4(~0u, ~0u, ~0u, ~0u);
+        if (bits) {
+          x[v] = __ldg(reinterpret_cast<const uint4*>(L + (int64_t)r[v] * W) + q);
+          x[v].x |= ~nibble_bytes(bits & 0xFu);
+          x[v].y |= ~nibble_bytes((bits >> 4) & 0xFu);
+          x[v].z |= ~nibble_bytes((bits >> 8) & 0xFu);
+          x[v].w |= ~nibble_bytes((bits >> 12) & 0xFu);
         }
       }
-    }
-    uint32_t* row = tile + threadIdx.x * SW;
 #pragma unroll
-    for (int q = 0; q < CHUNKS; ++q) {
-      row[4 * q] = x[q].x;
-      row[4 * q + 1] = x[q].y;
-      row[4 * q + 2] = x[q].z;
-      row[4 * q + 3] = x[q].w;
+      for (int i = 0; i < 4; ++i) {
+        const int lb = 4 * (4 * q + i);  // lanes lb .. lb + 3
+        if (lb >= nroots) break;
+        uint32_t a[4], c[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) a[v] = i == 0 ? x[v].x : i == 1 ? x[v].y : i == 2 ? x[v].z : x[v].w;
+        transpose4x4(a, c);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (lb + j < nroots) *reinterpret_cast<uint32_t*>(out + (int64_t)(lb + j) * nolv + u0) = c[j];
+      }
     }
-    __syncthreads();
-    // item = (lane, 32-vertex segment); each warp takes items in turn
-    constexpr int SEGS = TR_TILE / 32;
-    for (int item = warp; item < nroots * SEGS; item += TR_TILE / 32) {
-      const int l = item / SEGS, t = (item % SEGS) * 32 + lane_id;
-      const int64_t v = base + t;
-      if (v < nolv) out[(int64_t)l * nolv + v] = (uint8_t)(tile[t * SW + (l >> 2)] >> (8 * (l & 3)));
-    }
-    __syncthreads();
   }
 }
 
@@ -951,10 +960,10 @@ static int ms_enqueue_batch(g500_msbfs* m, int b, cudaStream_t s) {
   else if (W == 64) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<2>, p));
   else G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<4>, p));
   uint8_t* out = m->out + (int64_t)b * W * g->nolv;
-  const unsigned tg = (unsigned)std::min<int64_t>(ceil_div(g->nolv, TR_TILE), (int64_t)num_sms() * 8);
-  if (W == 32) ms_transpose_kernel<1><<<tg, TR_TILE, 0, s>>>(m->L, m->V, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
-  else if (W == 64) ms_transpose_kernel<2><<<tg, TR_TILE, 0, s>>>(m->L, m->V, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
-  else ms_transpose_kernel<4><<<tg, TR_TILE, 0, s>>>(m->L, m->V, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
+  const unsigned tg = (unsigned)std::min<int64_t>(ceil_div(g->nolv, 4 * TR_BLOCK), (int64_t)num_sms() * 8);
+  if (W == 32) ms_transpose_kernel<1><<<tg, TR_BLOCK, 0, s>>>(m->L, m->V, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
+  else if (W == 64) ms_transpose_kernel<2><<<tg, TR_BLOCK, 0, s>>>(m->L, m->V, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
+  else ms_transpose_kernel<4><<<tg, TR_BLOCK, 0, s>>>(m->L, m->V, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
   ms_root_fixup_kernel<<<1, MS_MAX_LANES, 0, s>>>(m->roots_dev + b * MS_MAX_LANES, m->nroots_dev + b, g->nolv, out);
   G500_CUDA(cudaGetLastError());
   return G500_OK;
