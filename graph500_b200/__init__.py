@@ -83,6 +83,35 @@ class MsLevel(C.Structure):
                 ("expand_ms", C.c_double)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("max_batch", C.c_int32), ("max_workers_per_graph", C.c_int32), ("mode", C.c_int32),
+                ("vertices_per_block", C.c_int32), ("hbm_reserve_bytes", C.c_uint64), ("alpha", C.c_double)]
+
+
+class QueryResult(C.Structure):
+    _fields_ = [("id", C.c_int64), ("tag", C.c_uint64), ("graph", C.c_int32), ("status", C.c_int32),
+                ("root", C.c_int64), ("reached", C.c_int64), ("nedge", C.c_int64), ("arrival_us", C.c_double),
+                ("start_us", C.c_double), ("done_us", C.c_double), ("batch_size", C.c_int32),
+                ("lane_width", C.c_int32)]
+
+
+class ServerInfo(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("finished", C.c_int64), ("launches", C.c_int64),
+                ("queries_launched", C.c_int64), ("workers", C.c_int32), ("max_in_flight", C.c_int32),
+                ("block_capacity", C.c_int32), ("pad", C.c_int32)]
+
+
+class ServeReport(C.Structure):
+    _fields_ = [("rate_qps", C.c_double), ("queries", C.c_int64), ("failed", C.c_int64), ("wall_s", C.c_double),
+                ("achieved_qps", C.c_double), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("mean_ms", C.c_double), ("max_ms", C.c_double), ("gteps", C.c_double), ("nedge", C.c_int64),
+                ("mean_batch", C.c_double), ("launches", C.c_int64), ("max_in_flight", C.c_int32),
+                ("workers", C.c_int32)]
+
+
+SERVE_BATCHED, SERVE_PLAIN = 0, 1
+
+
 class ValidateReport(C.Structure):
     _fields_ = [("range_errors", C.c_int64), ("root_errors", C.c_int64), ("self_parent_errors", C.c_int64),
                 ("depth_errors", C.c_int64), ("edge_errors", C.c_int64),
@@ -140,6 +169,21 @@ def lib() -> C.CDLL:
         "g500_msbfs_root_stats": ([P, P, P], i32),
         "g500_msbfs_device_levels": ([P, C.POINTER(P)], i32),
         "g500_msbfs_level_info": ([P, i32, C.POINTER(MsLevel), i32, C.POINTER(i32)], i32),
+        "g500_msbfs_launch": ([P, P, i32], i32),
+        "g500_msbfs_poll": ([P, C.POINTER(i32)], i32),
+        "g500_msbfs_wait": ([P, C.POINTER(MsStats)], i32),
+        "g500_msbfs_set_root_stats": ([P, i32], i32),
+        "g500_msbfs_set_grid": ([P, i32], i32),
+        "g500_msbfs_get_grid": ([P, i32, C.POINTER(i32), C.POINTER(i32)], i32),
+        "g500_msbfs_workspace_bytes": ([P, C.POINTER(u64)], i32),
+        "g500_server_default_config": ([C.POINTER(ServerConfig)], i32),
+        "g500_server_create": ([P, i32, C.POINTER(ServerConfig), C.POINTER(P)], i32),
+        "g500_server_submit": ([P, i32, i64, u64, P, C.POINTER(i64)], i32),
+        "g500_server_poll": ([P, C.POINTER(QueryResult), i32, C.POINTER(i32), i32], i32),
+        "g500_server_drain": ([P, i32], i32),
+        "g500_server_info": ([P, C.POINTER(ServerInfo)], i32),
+        "g500_server_run_poisson": ([P, C.c_double, i64, u64, i64, C.POINTER(ServeReport)], i32),
+        "g500_server_destroy": ([P], i32),
         "g500_msbfs_autotune": ([P, P, i32, i32, C.POINTER(MsTune)], i32),
         "g500_msbfs_destroy": ([P], i32),
         "g500_validate_noalloc": ([P, i64, i64, i64, i64, P, P, C.POINTER(i64), C.POINTER(i32),
@@ -452,6 +496,40 @@ class MultiSourceBFS:
         check(lib().g500_msbfs_root_stats(self.h, reached.ctypes.data, nedge.ctypes.data))
         return reached, nedge
 
+    def launch(self, roots) -> None:
+        """Enqueue a call and return at once (g500_msbfs_launch); levels stay on the device."""
+        self._launched = np.ascontiguousarray(roots, dtype=np.int64)
+        check(lib().g500_msbfs_launch(self.h, self._launched.ctypes.data, len(self._launched)))
+
+    def poll(self) -> bool:
+        done = C.c_int32()
+        check(lib().g500_msbfs_poll(self.h, C.byref(done)))
+        return bool(done.value)
+
+    def wait(self) -> MsStats:
+        st = MsStats()
+        check(lib().g500_msbfs_wait(self.h, C.byref(st)))
+        return st
+
+    def set_root_stats(self, on: bool = True) -> None:
+        check(lib().g500_msbfs_set_root_stats(self.h, int(on)))
+
+    def set_grid(self, blocks: int = 0) -> None:
+        check(lib().g500_msbfs_set_grid(self.h, blocks))
+
+    def grid(self, lane_width: int = 64) -> tuple[int, int]:
+        b, mx = C.c_int32(), C.c_int32()
+        check(lib().g500_msbfs_get_grid(self.h, lane_width, C.byref(b), C.byref(mx)))
+        return b.value, mx.value
+
+    def device_levels(self, nroots: int):
+        """The device output of the last call as a (nroots, pred_size) uint8 torch tensor view."""
+        import torch
+        p = C.c_void_p()
+        check(lib().g500_msbfs_device_levels(self.h, C.byref(p)))
+        n = nroots * self.graph.pred_size()
+        return _device_u8(p.value, n).view(nroots, self.graph.pred_size())
+
     def level_info(self, batch: int = 0) -> list[dict]:
         """Per level of launch `batch` of the last run: direction, discovered
         (vertex, root) pairs and device milliseconds."""
@@ -507,3 +585,82 @@ def levels_from_pred(pred: np.ndarray) -> np.ndarray:
     lv = ((pred >> 48) & 0xFFFF).astype(np.uint16)
     lv[pred == -1] = 0xFFFF
     return lv
+
+
+def _device_u8(ptr: int, n: int):
+    """A torch uint8 CUDA tensor over n bytes of library-owned device memory (no copy)."""
+    import torch
+
+    class _Arr:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False), "version": 3}
+    return torch.as_tensor(_Arr(), device="cuda")
+
+
+# ---------------------------------------------------------------------------
+# serving
+# ---------------------------------------------------------------------------
+class Server:
+    """Request loop over resident graphs (g500_server_*): queries are batched
+    into multi-source launches as they arrive (continuous batching)."""
+
+    def __init__(self, graphs, **config):
+        cfg = ServerConfig()
+        check(lib().g500_server_default_config(C.byref(cfg)))
+        for k, v in config.items():
+            if not hasattr(cfg, k):
+                raise TypeError(f"unknown server option {k}")
+            setattr(cfg, k, v)
+        self.graphs = list(graphs)
+        arr = (C.c_void_p * len(self.graphs))(*[g.h.value if isinstance(g.h, C.c_void_p) else g.h
+                                                 for g in self.graphs])
+        h = C.c_void_p()
+        check(lib().g500_server_create(arr, len(self.graphs), C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def submit(self, graph: int, root: int, tag: int = 0, levels=None) -> int:
+        """levels: None or a buffer of pred_size bytes (host or device) for the query's levels."""
+        ptr = None
+        if levels is not None:
+            if _nbytes(levels) < self.graphs[graph].pred_size():
+                raise ValueError("levels buffer smaller than pred_size bytes")
+            ptr, _ = _ptr(levels)
+        qid = C.c_int64()
+        check(lib().g500_server_submit(self.h, graph, int(root), tag, ptr, C.byref(qid)))
+        if levels is not None:
+            self._keep[qid.value] = levels
+        return qid.value
+
+    def poll(self, max_results: int = 1024, wait_us: int = 0) -> list[dict]:
+        buf = (QueryResult * max_results)()
+        n = C.c_int32()
+        check(lib().g500_server_poll(self.h, buf, max_results, C.byref(n), wait_us))
+        out = [{f[0]: getattr(buf[i], f[0]) for f in QueryResult._fields_} for i in range(n.value)]
+        for r in out:
+            self._keep.pop(r["id"], None)
+        return out
+
+    def drain(self, timeout_ms: int = 60000) -> None:
+        check(lib().g500_server_drain(self.h, timeout_ms))
+
+    def info(self) -> dict:
+        i = ServerInfo()
+        check(lib().g500_server_info(self.h, C.byref(i)))
+        return {f[0]: getattr(i, f[0]) for f in ServerInfo._fields_}
+
+    def run_poisson(self, rate_qps: float, num_queries: int, seed: int = 2026, warmup: int = 0) -> dict:
+        rep = ServeReport()
+        check(lib().g500_server_run_poisson(self.h, rate_qps, num_queries, seed, warmup, C.byref(rep)))
+        return {f[0]: getattr(rep, f[0]) for f in ServeReport._fields_}
+
+    def close(self) -> None:
+        if self.h is not None:
+            check(lib().g500_server_destroy(self.h))
+            self.h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -38,8 +38,8 @@
 
 namespace g500 {
 
-constexpr int BFS_THREADS = 256;
-constexpr int BFS_MIN_BLOCKS = 4;        // co-resident blocks per SM (64 registers, no spills)
+constexpr int BFS_THREADS = 512;
+constexpr int BFS_MIN_BLOCKS = 2;        // co-resident blocks per SM (64 registers, no spills)
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
 constexpr int BU_WORDS = 8;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
 constexpr int BU_SERIAL = 6;              // row entries a lane checks alone before the warp helps

@@ -175,3 +175,9 @@ struct g500_bfs {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int64_t last_root = -1;
 };
+
+namespace g500 {
+// g500_msbfs_launch that also copies each root's level row (pred_size bytes)
+// to root_dsts[i] when it is not null, before the launch's completion event.
+int msbfs_launch_to(g500_msbfs* m, const int64_t* roots, int nroots, uint8_t* const* root_dsts);
+}  // namespace g500

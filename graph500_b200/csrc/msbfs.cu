@@ -715,6 +715,20 @@ __global__ void __launch_bounds__(TR_BLOCK) ms_transpose_kernel(const uint8_t* _
   }
 }
 
+// a root outside the CSR range (no edges) reached only itself; its self-loop
+// occurrences are its edge count
+__global__ void ms_root_stats_fixup_kernel(const int64_t* roots, const int* nroots_dev, const uint32_t* reorder,
+                                           int64_t nlv, const uint32_t* endp, unsigned long long* reached,
+                                           unsigned long long* e2) {
+  const int i = threadIdx.x;
+  if (i >= *nroots_dev) return;
+  const uint32_t r = reorder[roots[i]];
+  if ((int64_t)r >= nlv) {
+    reached[i] = 1;
+    e2[i] = endp[r];
+  }
+}
+
 // every root is its own level 0 (also a root outside the CSR range)
 __global__ void ms_root_fixup_kernel(const int64_t* roots, const int* nroots_dev, int64_t nolv, uint8_t* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -809,7 +823,13 @@ struct g500_msbfs {
   int64_t* staging = nullptr;                         // pinned: [4][128] roots + [4] counts
   MsCtl* h_ctl = nullptr;                             // pinned [4]
   unsigned long long* stats_dev = nullptr;            // [2][128]
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  unsigned long long* h_stats = nullptr;              // pinned [2][128]: reached, 2 * nedge per lane
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_done = nullptr;
+  unsigned grid_full[3] = {0, 0, 0};                  // the whole device's co-resident blocks
+  int want_stats = 0;                                 // root statistics enqueued with every one-launch call
+  int in_flight = 0, fl_batches = 0, fl_stats = 0, stats_valid = 0;
+  std::vector<int64_t> fl_roots, last_roots;
+  std::chrono::steady_clock::time_point t_launch;
   cudaGraphExec_t graphs[3][4] = {};                  // [log2(W/32)][batch]
   uint32_t* deg = nullptr;                            // [nlv] row lengths
   uint2* hub_tab = nullptr;                           // pull: [nhub_chunks] (hub row, chunk index)
@@ -850,8 +870,10 @@ static int ms_free(g500_msbfs* m) {
   dev_free(m->push_tab);
   if (m->staging) cudaFreeHost(m->staging);
   if (m->h_ctl) cudaFreeHost(m->h_ctl);
+  if (m->h_stats) cudaFreeHost(m->h_stats);
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
+  if (m->ev_done) cudaEventDestroy(m->ev_done);
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
   return G500_OK;
@@ -1000,6 +1022,10 @@ extern "C" int g500_msbfs_create(g500_graph* g, g500_msbfs** out) {
   if (st == G500_OK) chk(cudaHostAlloc(&m->h_ctl, sizeof(MsCtl) * 4, cudaHostAllocDefault), "cudaHostAlloc");
   chk(cudaEventCreate(&m->ev0), "cudaEventCreate");
   chk(cudaEventCreate(&m->ev1), "cudaEventCreate");
+  chk(cudaEventCreateWithFlags(&m->ev_done, cudaEventDisableTiming), "cudaEventCreate");
+  if (st == G500_OK)
+    chk(cudaHostAlloc(&m->h_stats, sizeof(unsigned long long) * 2 * MS_MAX_LANES, cudaHostAllocDefault),
+        "cudaHostAlloc");
   if (st == G500_OK) st = ms_build_hubs(m, MS_HUB_DEG, MS_HUB_CHUNK, &m->hub_tab, &m->nhub_chunks);
   if (st == G500_OK) st = ms_build_hubs(m, MS_PUSH_HUB_DEG, MS_PUSH_CHUNK, &m->push_tab, &m->npush_chunks);
   const void* kernels[3] = {ms_kernel_ptr<1>(), ms_kernel_ptr<2>(), ms_kernel_ptr<4>()};
@@ -1007,7 +1033,7 @@ extern "C" int g500_msbfs_create(g500_graph* g, g500_msbfs** out) {
     int per_sm = 0;
     chk(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernels[i], MS_THREADS, 0), "occupancy");
     if (st == G500_OK && per_sm <= 0) st = set_error(G500_E_DEVICE, "multi-source kernel cannot be co-scheduled");
-    m->grid[i] = (unsigned)(num_sms() * std::max(per_sm, 1));
+    m->grid[i] = m->grid_full[i] = (unsigned)(num_sms() * std::max(per_sm, 1));
   }
   if (st != G500_OK) {
     ms_free(m);
@@ -1022,16 +1048,40 @@ extern "C" int g500_msbfs_set_params(g500_msbfs* m, int lane_width, double alpha
   if (lane_width != 32 && lane_width != 64 && lane_width != 128)
     return set_error(G500_E_INVAL, "lane width %d not 32, 64 or 128", lane_width);
   if (!(alpha > 0)) return set_error(G500_E_INVAL, "alpha must be > 0");
-  if (lane_width != m->lane_width || alpha != m->alpha) ms_drop_graphs(m);
+  if (alpha != m->alpha) ms_drop_graphs(m);  // graphs are kept per lane width; alpha is captured in them
   m->lane_width = lane_width;
   m->alpha = alpha;
   m->use_graph = use_cuda_graph ? 1 : 0;
   return G500_OK;
 }
 
-extern "C" int g500_msbfs_run(g500_msbfs* m, const int64_t* roots, int nroots, uint8_t* levels, int levels_on_device,
-                              g500_msbfs_stats* stats) {
+// Per-lane reached / 2*nedge of the last launch into h_stats (enqueued on s).
+static int ms_enqueue_stats(g500_msbfs* m, int nroots, cudaStream_t s) {
+  g500_graph* g = m->g;
+  G500_CUDA(cudaMemsetAsync(m->stats_dev, 0, sizeof(unsigned long long) * 2 * MS_MAX_LANES, s));
+  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(std::max<int64_t>(g->nlv, 1), 256), num_sms() * 8);
+  const int W = m->lane_width;
+  unsigned long long* r = m->stats_dev;
+  unsigned long long* e = m->stats_dev + MS_MAX_LANES;
+  if (g->nlv > 0) {
+    if (W == 32) ms_stats_kernel<1><<<grid, 256, 0, s>>>(m->V, g->d_endp, g->nlv, nroots, r, e);
+    else if (W == 64) ms_stats_kernel<2><<<grid, 256, 0, s>>>(m->V, g->d_endp, g->nlv, nroots, r, e);
+    else ms_stats_kernel<4><<<grid, 256, 0, s>>>(m->V, g->d_endp, g->nlv, nroots, r, e);
+  }
+  ms_root_stats_fixup_kernel<<<1, MS_MAX_LANES, 0, s>>>(m->roots_dev, m->nroots_dev, g->d_reorder, g->nlv, g->d_endp,
+                                                        r, e);
+  G500_CUDA(cudaGetLastError());
+  G500_CUDA(cudaMemcpyAsync(m->h_stats, m->stats_dev, sizeof(unsigned long long) * 2 * MS_MAX_LANES,
+                            cudaMemcpyDeviceToHost, s));
+  return G500_OK;
+}
+
+// Enqueue a whole call (every launch, the optional level copy, the control
+// blocks' copy back, the optional root statistics) and record ev_done.
+static int ms_launch(g500_msbfs* m, const int64_t* roots, int nroots, uint8_t* levels, int levels_on_device,
+                     uint8_t* const* root_dsts = nullptr) {
   if (!m || !roots) return set_error(G500_E_INVAL, "null argument");
+  if (m->in_flight) return set_error(G500_E_STATE, "the previous launch has not been waited for");
   g500_graph* g = m->g;
   if (nroots < 1 || nroots > MS_MAX_LANES)
     return set_error(G500_E_INVAL, "%d roots; 1..%d per call", nroots, MS_MAX_LANES);
@@ -1039,7 +1089,7 @@ extern "C" int g500_msbfs_run(g500_msbfs* m, const int64_t* roots, int nroots, u
     if (roots[i] < 0 || roots[i] >= g->nolv)
       return set_error(G500_E_INVAL, "root %lld outside [0, %lld)", (long long)roots[i], (long long)g->nolv);
   G500_CUDA(cudaSetDevice(g->device));
-  auto t0 = std::chrono::steady_clock::now();
+  m->t_launch = std::chrono::steady_clock::now();
   const int W = m->lane_width;
   const int ni = nw_index(W);
   const int batches = (nroots + W - 1) / W;
@@ -1080,10 +1130,32 @@ extern "C" int g500_msbfs_run(g500_msbfs* m, const int64_t* roots, int nroots, u
     G500_CUDA(cudaMemcpyAsync(levels, m->out, (size_t)nroots * g->nolv,
                               levels_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
   }
+  if (root_dsts)
+    for (int i = 0; i < nroots; ++i)
+      if (root_dsts[i])
+        G500_CUDA(cudaMemcpyAsync(root_dsts[i], m->out + (int64_t)i * g->nolv, (size_t)g->nolv, cudaMemcpyDefault, s));
   G500_CUDA(cudaMemcpyAsync(m->h_ctl, m->ctl, sizeof(MsCtl) * batches, cudaMemcpyDeviceToHost, s));
-  G500_CUDA(cudaStreamSynchronize(s));
-  m->last_nroots = nroots;
+  m->fl_stats = m->want_stats && batches == 1;
+  if (m->fl_stats) G500_TRY(ms_enqueue_stats(m, nroots, s));
+  G500_CUDA(cudaEventRecord(m->ev_done, s));
+  m->fl_roots.assign(roots, roots + nroots);
+  m->fl_batches = batches;
+  m->in_flight = 1;
+  return G500_OK;
+}
+
+// Wait for the launch in flight and report it.
+static int ms_complete(g500_msbfs* m, g500_msbfs_stats* stats) {
+  if (!m->in_flight) return set_error(G500_E_STATE, "no launch in flight");
+  G500_CUDA(cudaSetDevice(m->g->device));
+  m->in_flight = 0;
+  cudaError_t ce = cudaEventSynchronize(m->ev_done);
+  if (ce != cudaSuccess) return cuda_error(ce, "cudaEventSynchronize", __FILE__, __LINE__);
+  const int batches = m->fl_batches;
+  m->last_roots = m->fl_roots;
+  m->last_nroots = (int)m->fl_roots.size();
   m->last_batches = batches;
+  m->stats_valid = m->fl_stats;
   unsigned err = 0;
   for (int b = 0; b < batches; ++b) err |= m->h_ctl[b].bar.err;
   if (err & GRID_ERR_TIMEOUT) return set_error(G500_E_TIMEOUT, "grid barrier wait gave up (bounded spin)");
@@ -1093,8 +1165,8 @@ extern "C" int g500_msbfs_run(g500_msbfs* m, const int64_t* roots, int nroots, u
     G500_CUDA(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
     memset(stats, 0, sizeof(*stats));
     stats->device_ms = ms;
-    stats->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    stats->lane_width = W;
+    stats->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - m->t_launch).count();
+    stats->lane_width = m->lane_width;
     stats->batches = batches;
     for (int b = 0; b < batches; ++b) {
       stats->num_levels = std::max<int32_t>(stats->num_levels, (int32_t)m->h_ctl[b].num_levels);
@@ -1103,46 +1175,102 @@ extern "C" int g500_msbfs_run(g500_msbfs* m, const int64_t* roots, int nroots, u
       if (c.t_init_ns >= c.t0_ns) stats->init_ms += (double)(c.t_init_ns - c.t0_ns) * 1e-6;
       if (c.t_end_ns >= c.t_init_ns) stats->search_ms += (double)(c.t_end_ns - c.t_init_ns) * 1e-6;
     }
-    stats->kernel_launches = 3 * batches;
+    stats->kernel_launches = 3 * batches + (m->fl_stats ? 2 : 0);
   }
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_run(g500_msbfs* m, const int64_t* roots, int nroots, uint8_t* levels, int levels_on_device,
+                              g500_msbfs_stats* stats) {
+  G500_TRY(ms_launch(m, roots, nroots, levels, levels_on_device));
+  return ms_complete(m, stats);
+}
+
+extern "C" int g500_msbfs_launch(g500_msbfs* m, const int64_t* roots, int nroots) {
+  return ms_launch(m, roots, nroots, nullptr, 0);
+}
+
+namespace g500 {
+int msbfs_launch_to(g500_msbfs* m, const int64_t* roots, int nroots, uint8_t* const* root_dsts) {
+  return ms_launch(m, roots, nroots, nullptr, 0, root_dsts);
+}
+}  // namespace g500
+
+extern "C" int g500_msbfs_poll(g500_msbfs* m, int* done) {
+  if (!m || !done) return set_error(G500_E_INVAL, "null argument");
+  if (!m->in_flight) return set_error(G500_E_STATE, "no launch in flight");
+  const cudaError_t e = cudaEventQuery(m->ev_done);
+  if (e == cudaSuccess) {
+    *done = 1;
+    return G500_OK;
+  }
+  if (e == cudaErrorNotReady) {
+    *done = 0;
+    return G500_OK;
+  }
+  return cuda_error(e, "cudaEventQuery", __FILE__, __LINE__);
+}
+
+extern "C" int g500_msbfs_wait(g500_msbfs* m, g500_msbfs_stats* stats) {
+  if (!m) return set_error(G500_E_INVAL, "null handle");
+  return ms_complete(m, stats);
+}
+
+extern "C" int g500_msbfs_set_root_stats(g500_msbfs* m, int on) {
+  if (!m) return set_error(G500_E_INVAL, "null handle");
+  m->want_stats = on ? 1 : 0;
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_set_grid(g500_msbfs* m, int blocks) {
+  if (!m) return set_error(G500_E_INVAL, "null handle");
+  if (blocks < 0) return set_error(G500_E_INVAL, "negative block count");
+  if (m->in_flight) return set_error(G500_E_STATE, "a launch is in flight");
+  for (int i = 0; i < 3; ++i) {
+    const unsigned want = blocks == 0 ? m->grid_full[i] : std::min<unsigned>((unsigned)blocks, m->grid_full[i]);
+    if (want != m->grid[i]) {
+      ms_drop_graphs(m);
+      m->grid[i] = want;
+    }
+  }
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_get_grid(const g500_msbfs* m, int lane_width, int* blocks, int* max_blocks) {
+  if (!m) return set_error(G500_E_INVAL, "null handle");
+  if (lane_width != 32 && lane_width != 64 && lane_width != 128)
+    return set_error(G500_E_INVAL, "lane width %d not 32, 64 or 128", lane_width);
+  if (blocks) *blocks = (int)m->grid[nw_index(lane_width)];
+  if (max_blocks) *max_blocks = (int)m->grid_full[nw_index(lane_width)];
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_workspace_bytes(const g500_graph* g, uint64_t* bytes) {
+  if (!g || !bytes) return set_error(G500_E_INVAL, "null argument");
+  const uint64_t nlv = (uint64_t)std::max<int64_t>(g->nlv, 1);
+  // V, F, N (4 words each), L (128 bytes), row lengths, output rows, with room
+  // for the hub tables and control blocks
+  *bytes = nlv * (3 * 16 + MS_MAX_LANES + 4) + (uint64_t)MS_MAX_LANES * (uint64_t)g->nolv + (16ull << 20) +
+           (uint64_t)g->nge / 64;
   return G500_OK;
 }
 
 extern "C" int g500_msbfs_root_stats(g500_msbfs* m, int64_t* reached, int64_t* nedge) {
   if (!m) return set_error(G500_E_INVAL, "null handle");
+  if (m->in_flight) return set_error(G500_E_STATE, "a launch is in flight");
   if (m->last_nroots == 0) return set_error(G500_E_STATE, "no run yet");
   if (m->last_batches != 1)
     return set_error(G500_E_STATE, "root statistics need the last run to fit one launch (roots <= lane width)");
-  g500_graph* g = m->g;
-  G500_CUDA(cudaSetDevice(g->device));
-  cudaStream_t s = m->stream;
-  G500_CUDA(cudaMemsetAsync(m->stats_dev, 0, sizeof(unsigned long long) * 2 * MS_MAX_LANES, s));
-  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(std::max<int64_t>(g->nlv, 1), 256), num_sms() * 8);
-  const int W = m->lane_width, n = m->last_nroots;
-  unsigned long long* r = m->stats_dev;
-  unsigned long long* e = m->stats_dev + MS_MAX_LANES;
-  if (W == 32) ms_stats_kernel<1><<<grid, 256, 0, s>>>(m->V, g->d_endp, g->nlv, n, r, e);
-  else if (W == 64) ms_stats_kernel<2><<<grid, 256, 0, s>>>(m->V, g->d_endp, g->nlv, n, r, e);
-  else ms_stats_kernel<4><<<grid, 256, 0, s>>>(m->V, g->d_endp, g->nlv, n, r, e);
-  G500_CUDA(cudaGetLastError());
-  unsigned long long h[2 * MS_MAX_LANES];
-  G500_CUDA(cudaMemcpyAsync(h, m->stats_dev, sizeof(h), cudaMemcpyDeviceToHost, s));
-  G500_CUDA(cudaStreamSynchronize(s));
-  for (int i = 0; i < n; ++i) {
-    if (reached) reached[i] = (int64_t)h[i];
-    if (nedge) nedge[i] = (int64_t)(h[MS_MAX_LANES + i] / 2);
+  G500_CUDA(cudaSetDevice(m->g->device));
+  const int n = m->last_nroots;
+  if (!m->stats_valid) {
+    G500_TRY(ms_enqueue_stats(m, n, m->stream));
+    G500_CUDA(cudaStreamSynchronize(m->stream));
+    m->stats_valid = 1;
   }
-  // a root outside the CSR range (no edges) reached only itself
-  std::vector<int64_t> rts(m->staging, m->staging + n);
   for (int i = 0; i < n; ++i) {
-    uint32_t rr = 0;
-    G500_CUDA(cudaMemcpy(&rr, g->d_reorder + rts[(size_t)i], sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    if ((int64_t)rr >= g->nlv) {
-      uint32_t ep = 0;
-      G500_CUDA(cudaMemcpy(&ep, g->d_endp + rr, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-      if (reached) reached[i] = 1;
-      if (nedge) nedge[i] = ep / 2;
-    }
+    if (reached) reached[i] = (int64_t)m->h_stats[i];
+    if (nedge) nedge[i] = (int64_t)(m->h_stats[MS_MAX_LANES + i] / 2);
   }
   return G500_OK;
 }

@@ -256,9 +256,101 @@ typedef struct g500_msbfs_level {
 /* Copies up to max_levels records of launch `batch` of the last run into out;
  * *num_levels receives the launch's level count. */
 int g500_msbfs_level_info(const g500_msbfs* m, int batch, g500_msbfs_level* out, int max_levels, int* num_levels);
+/* Asynchronous form of g500_msbfs_run for callers that overlap several
+ * handles (the serving loop): launch enqueues the whole call on the handle's
+ * stream and returns; poll reports whether it finished; wait blocks until it
+ * has, checks the device status and fills stats.  One launch in flight per
+ * handle; levels stay on the device (g500_msbfs_device_levels). */
+int g500_msbfs_launch(g500_msbfs* m, const int64_t* roots, int num_roots);
+int g500_msbfs_poll(g500_msbfs* m, int* done);
+int g500_msbfs_wait(g500_msbfs* m, g500_msbfs_stats* stats);
+/* on != 0: every call that fits one launch also computes the per-root
+ * statistics of g500_msbfs_root_stats on the device, in the same stream. */
+int g500_msbfs_set_root_stats(g500_msbfs* m, int on);
+/* Blocks per launch (0 = every co-resident block of the device).  Fewer
+ * blocks leave SMs to launches of other handles running at the same time. */
+int g500_msbfs_set_grid(g500_msbfs* m, int blocks);
+int g500_msbfs_get_grid(const g500_msbfs* m, int lane_width, int* blocks, int* max_blocks);
+/* Device memory one handle on this graph allocates (an upper bound). */
+int g500_msbfs_workspace_bytes(const g500_graph* g, uint64_t* bytes);
 /* Autotuner over lane width and alpha on sample roots (kept on the handle). */
 int g500_msbfs_autotune(g500_msbfs* m, const int64_t* roots, int num_roots, int reps, g500_msbfs_tune* out);
 int g500_msbfs_destroy(g500_msbfs* m);
+
+/* ------------------------------------------------------------- serving */
+/* A request loop over several resident graphs: BFS queries (graph, root) are
+ * admitted as they arrive, batched into multi-source launches while earlier
+ * launches run (continuous batching), and overlap on the device on separate
+ * streams.  A new launch slot (a g500_msbfs workspace) is created only while
+ * the device keeps hbm_reserve_bytes free.  No counterpart in the reference,
+ * which runs one root at a time (main.cc:105-160).  Each query's levels equal
+ * the plain BFS's (pred >> 48) for its root, alone or in any mix.  The graphs
+ * stay owned by the caller and must outlive the server. */
+typedef struct g500_server g500_server;
+enum g500_serve_mode { G500_SERVE_BATCHED = 0, G500_SERVE_PLAIN = 1 };
+
+typedef struct g500_server_config {
+  int32_t max_batch;             /* queries per launch, 1..128 */
+  int32_t max_workers_per_graph; /* concurrent launches per graph */
+  int32_t mode;                  /* G500_SERVE_BATCHED, or G500_SERVE_PLAIN: one g500_bfs_run per query */
+  int32_t vertices_per_block;    /* grid of a graph's launches: ceil(num_local_verts / this), >= 16 blocks */
+  uint64_t hbm_reserve_bytes;    /* free device memory a new launch slot must leave */
+  double alpha;                  /* multi-source direction threshold (g500_msbfs_set_params) */
+} g500_server_config;
+
+typedef struct g500_query_result {
+  int64_t id;
+  uint64_t tag;
+  int32_t graph;
+  int32_t status;                /* G500_OK or the error of its launch */
+  int64_t root;
+  int64_t reached;               /* vertices with a level */
+  int64_t nedge;                 /* input edges inside the reached component */
+  double arrival_us;             /* host steady clock, microseconds since the server was created */
+  double start_us;               /* its launch */
+  double done_us;                /* seen complete by the server */
+  int32_t batch_size;            /* queries in its launch */
+  int32_t lane_width;
+} g500_query_result;
+
+typedef struct g500_server_info_t {
+  int64_t submitted, finished, launches, queries_launched;
+  int32_t workers, max_in_flight, block_capacity, pad;
+} g500_server_info_t;
+
+typedef struct g500_serve_report {
+  double rate_qps;               /* offered Poisson rate */
+  int64_t queries;               /* measured (after warm-up) and completed */
+  int64_t failed;
+  double wall_s;                 /* first measured arrival to last completion */
+  double achieved_qps;
+  double p50_ms, p99_ms, mean_ms, max_ms;  /* completion - arrival */
+  double gteps;                  /* sum of nedge / wall */
+  int64_t nedge;
+  double mean_batch;             /* queries per launch */
+  int64_t launches;
+  int32_t max_in_flight;         /* launches running at once */
+  int32_t workers;               /* launch slots created so far */
+} g500_serve_report;
+
+int g500_server_default_config(g500_server_config* cfg);
+int g500_server_create(g500_graph* const* graphs, int num_graphs, const g500_server_config* cfg, g500_server** out);
+/* levels_out: NULL, or pred_size bytes that receive the query's levels (uint8,
+ * original ids, 255 unreached) before it completes; pinned host memory
+ * (g500_host_alloc) or device memory keeps the copy asynchronous. */
+int g500_server_submit(g500_server* s, int graph, int64_t root, uint64_t tag, uint8_t* levels_out, int64_t* id);
+/* Up to max_results completed queries (waiting up to wait_us for the first). */
+int g500_server_poll(g500_server* s, g500_query_result* out, int max_results, int* num, int wait_us);
+/* Wait until every submitted query has completed. */
+int g500_server_drain(g500_server* s, int timeout_ms);
+int g500_server_info(g500_server* s, g500_server_info_t* info);
+/* Open-loop load: num_queries Poisson arrivals at rate_qps, each on a graph
+ * chosen uniformly and a root chosen uniformly among vertices with at least
+ * one edge (splitmix64 stream from seed); latency statistics skip the first
+ * `warmup` queries. */
+int g500_server_run_poisson(g500_server* s, double rate_qps, int64_t num_queries, uint64_t seed, int64_t warmup,
+                            g500_serve_report* rep);
+int g500_server_destroy(g500_server* s);
 
 /* Validation that allocates nothing, for callers that cannot call cudaMalloc
  * (a host framework owning all device memory through its own arena or caching

@@ -29,17 +29,21 @@ def test_symbols_are_plain_c(g500):
 def test_struct_layout_matches_header(g500, tmp_path):
     """ctypes mirrors have the sizes the C compiler gives the header's structs."""
     src = tmp_path / "sz.c"
-    src.write_text('#include "g500.h"\n#include <stdio.h>\nint main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
+    src.write_text('#include "g500.h"\n#include <stdio.h>\nint main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
                    'sizeof(g500_graph_info),sizeof(g500_level_stats),sizeof(g500_bfs_stats),'
                    'sizeof(g500_validate_report),sizeof(g500_packed_edge),sizeof(g500_tune_result),'
-                   'sizeof(g500_msbfs_stats),sizeof(g500_msbfs_tune),sizeof(g500_msbfs_level));return 0;}\n')
+                   'sizeof(g500_msbfs_stats),sizeof(g500_msbfs_tune),sizeof(g500_msbfs_level),'
+                   'sizeof(g500_server_config),sizeof(g500_query_result),sizeof(g500_server_info_t),'
+                   'sizeof(g500_serve_report));return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True,
                    env={k: v for k, v in os.environ.items() if k not in ("CC", "CXX")})
     sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     assert sizes == [ctypes.sizeof(g500.GraphInfo), ctypes.sizeof(g500.LevelStats), ctypes.sizeof(g500.BfsStats),
                      ctypes.sizeof(g500.ValidateReport), g500.EDGE_DTYPE.itemsize, ctypes.sizeof(g500.TuneResult),
-                     ctypes.sizeof(g500.MsStats), ctypes.sizeof(g500.MsTune), ctypes.sizeof(g500.MsLevel)]
+                     ctypes.sizeof(g500.MsStats), ctypes.sizeof(g500.MsTune), ctypes.sizeof(g500.MsLevel),
+                     ctypes.sizeof(g500.ServerConfig), ctypes.sizeof(g500.QueryResult), ctypes.sizeof(g500.ServerInfo),
+                     ctypes.sizeof(g500.ServeReport)]
 
 
 def test_scramble_values_match_oracle(g500, oracle_mod):
