@@ -54,6 +54,15 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-roots", type=int, default=8, help="roots in the bounded CPU-baseline sample")
     ap.add_argument("--ref-roots-per-step", type=int, default=4)
+    ap.add_argument("--extra-scales", default="24,26",
+                    help="graph sizes measured beside the main one (plain + batched), comma-separated; '' for none")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-scales", default="18,20,22,24")
+    ap.add_argument("--serve-rates", default="1000,3000,10000,30000,100000")
+    ap.add_argument("--serve-queries", type=int, default=10000)
+    ap.add_argument("--serve-warmup", type=int, default=1000)
+    ap.add_argument("--serve-plain-queries", type=int, default=2000)
+    ap.add_argument("--serve-workers", type=int, default=2)
     return ap.parse_args()
 
 
@@ -248,6 +257,98 @@ def batched_arm(a, g5, torch, bfs, roots, nedge, pred_dev, local, reduce_max, re
             "parity": "levels of every root equal the plain BFS's (pred >> 48)"}
 
 
+def scale_section(a, g5, torch, scale, reduce_max, reduce_sum, barrier, peak) -> dict:
+    """Plain BFS and batched MS-BFS on another graph size (SCALE 24 is the
+    batched configuration, SCALE 26 the plain-at-scale one): 64 roots, every
+    root validated on the device (untimed), autotuned plain BFS timed with L2
+    flushed before each root, then the MS-BFS launch over the same roots with
+    each root's levels checked against the plain run."""
+    g = g5.Graph2DCSR.generate(scale, a.edgefactor, a.reorder)
+    gen_s, build_s = g.timings()
+    info = g.info
+    bfs = g5.BfsOnGPU(reorder_mode=a.reorder)
+    bfs.graph_ = g
+    bfs.prepare_bfs()
+    roots = g5.find_roots(g, a.roots)
+    tune = bfs.autotune(roots[:a.tune_roots], reps=2)
+    pred = torch.empty(info.pred_size, dtype=torch.int64, device="cuda")
+    nedge, model = [], []
+    bfs.set_params(tune["alpha"], tune["beta"], count_edges=True, policy=tune["policy"])
+    for r in roots:
+        bfs.run_bfs(int(r), pred)
+        ok, evc, rep = g5.validate_bfs_result(g, int(r), pred)
+        if not ok:
+            raise SystemExit(f"SCALE {scale}: validation failed for root {r}: {rep}")
+        nedge.append(evc)
+        model.append(sum(bytes_model(bfs.level_stats(), info.pred_size, info.num_local_verts)))
+    bfs.set_params(tune["alpha"], tune["beta"], count_edges=False, policy=tune["policy"])
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for r in roots[:8]:
+        bfs.run_bfs(int(r), pred)
+    barrier()
+    ts = []
+    for r in roots:
+        flush.zero_()
+        torch.cuda.synchronize()
+        ts.append(bfs.run_bfs(int(r), pred).device_ms)
+    barrier()
+    t_max = reduce_max(sum(ts) / 1000.0)
+    e_all = reduce_sum(float(sum(nedge)))
+    plain = e_all / t_max / 1e9
+    hm = 1.0 / (sum(t / 1000.0 / e for t, e in zip(ts, nedge)) / len(ts)) / 1e9
+    achieved = sum(model) / (sum(ts) / 1000.0) / 1e9
+    out = {"workload": f"Kronecker SCALE {scale} edgefactor {a.edgefactor}, VERTEX_REORDERING {a.reorder}, "
+                       f"{len(roots)} roots, all validated",
+           "plain_gteps": plain, "plain_harmonic_mean_gteps": hm, "plain_ms_per_root": sum(ts) / len(ts),
+           "plain_tuning": {k: tune[k] for k in ("policy", "alpha", "beta")},
+           "plain_roofline": {"bound": "hbm", "kernel": "bfs_persistent_kernel", "achieved": achieved, "peak": peak,
+                              "unit": "GB/s", "frac": achieved / peak,
+                              "bytes_per_launch": sum(model) / len(model)},
+           "graph": {"num_global_verts": info.num_global_verts, "num_global_edges": info.num_global_edges,
+                     "generation_s": gen_s, "construction_s": build_s}}
+    bat = batched_arm(a, g5, torch, bfs, roots, nedge, pred, 0, reduce_max, reduce_sum, barrier)
+    out["batched"] = {k: bat[k] for k in ("value", "unit", "lane_width", "alpha", "ms_per_step", "levels",
+                                          "pull_levels", "parity")}
+    out["batched"]["speedup_vs_plain"] = bat["value"] / plain if plain else None
+    bfs.close()
+    del pred, flush
+    torch.cuda.empty_cache()
+    return out
+
+
+def serving_arm(a, g5, torch, reduce_sum, barrier) -> dict:
+    """Resident graphs at SCALE 18/20/22/24, open-loop Poisson queries (uniform
+    graph, uniform degree>=1 root, splitmix64 seed 2026) at each rate; p50/p99
+    of completion - arrival after warm-up, aggregate GTEPS = sum of nedge /
+    wall.  Beside it, the same stream through plain per-query BFS."""
+    scales = [int(x) for x in a.serve_scales.split(",")]
+    graphs = [g5.Graph2DCSR.generate(sc, a.edgefactor, 2) for sc in scales]
+    out = {"workload": f"{len(graphs)} resident Kronecker graphs SCALE {'/'.join(map(str, scales))} "
+                       f"(edgefactor {a.edgefactor}, VERTEX_REORDERING 2), Poisson arrivals, up to 128 queries "
+                       f"per multi-source launch",
+           "queries_per_rate": a.serve_queries, "warmup_queries": a.serve_warmup, "rates": []}
+    srv = g5.Server(graphs, max_batch=128, max_workers_per_graph=a.serve_workers)
+    srv.run_poisson(1000.0, 400, seed=7)  # warm-up: captures the CUDA graphs of every lane width in use
+    for rate in [float(x) for x in a.serve_rates.split(",")]:
+        barrier()
+        rep = srv.run_poisson(rate, a.serve_queries + a.serve_warmup, seed=2026, warmup=a.serve_warmup)
+        rep["gteps_all_ranks"] = reduce_sum(rep["gteps"])
+        out["rates"].append(rep)
+    out["server"] = srv.info()
+    srv.close()
+    plain = g5.Server(graphs, mode=g5.SERVE_PLAIN)
+    plain.run_poisson(1000.0, 200, seed=7)
+    out["plain_per_query"] = []
+    for rate in [float(x) for x in a.serve_rates.split(",")]:
+        barrier()
+        rep = plain.run_poisson(rate, a.serve_plain_queries + 100, seed=2026, warmup=100)
+        out["plain_per_query"].append(rep)
+    plain.close()
+    for g in graphs:
+        g.close()
+    return out
+
+
 def our_arm(a):
     import torch
 
@@ -374,6 +475,11 @@ def our_arm(a):
 
     # batched multi-source BFS on the same graph and roots (one launch per 64 roots)
     batched = batched_arm(a, g5, torch, bfs, roots, nedge, pred_dev, local, reduce_max, reduce_sum, barrier)
+    peak, peak_kind = load_peaks()
+    sections = {}
+    for sc in [int(x) for x in a.extra_scales.split(",") if x]:
+        sections[f"scale{sc}"] = scale_section(a, g5, torch, sc, reduce_max, reduce_sum, barrier, peak)
+    serving = None if a.no_serving else serving_arm(a, g5, torch, reduce_sum, barrier)
 
     if rank != 0:
         bfs.close()
@@ -381,7 +487,6 @@ def our_arm(a):
             dist.destroy_process_group()
         return
 
-    peak, peak_kind = load_peaks()
     # One persistent kernel runs a whole BFS, so it is the dominant kernel:
     # algorithmic bytes of one BFS / its mean device time.
     runs = len(rec["t"])
@@ -411,6 +516,9 @@ def our_arm(a):
     }
     line["batched"] = batched
     line["batched"]["speedup_vs_plain"] = batched["value"] / value if value else None
+    line.update(sections)
+    if serving is not None:
+        line["serving"] = serving
     if world == 1 and not a.no_cpu_baseline:
         crec, err = run_ref_bench(a.scale, a.edgefactor, a.cpu_roots, 0, 1, a.cpu_roots, a.reorder)
         if crec is not None:
