@@ -7,11 +7,14 @@
 //          masks until all its unvisited lanes are found (bottom-up with
 //          early exit; VERTEX_REORDERING=2 puts hubs first in each row), or
 //   push   every frontier vertex ORs its mask into its neighbours' next masks
-//          (atomicOr, only the bits a neighbour still lacks),
+//          (atomicOr into N, only the bits a neighbour still lacks),
 //
-// followed by an apply pass (new = N & ~V; V |= new; F = new; levels).  Pull
-// or push is chosen per level from edge counts: pull when the new frontier's
-// degree sum exceeds (degree sum of vertices with unvisited lanes) / alpha.
+// followed by settling the new lanes (V |= new; next F = new; levels): a
+// pulling row settles itself, the hub rows (split across warps) and every
+// row after a push settle in a pass of their own.  The frontier masks are
+// double-buffered by level parity.  Pull or push is chosen per level from
+// edge counts: pull when the new frontier's degree sum exceeds (degree sum of
+// vertices with unvisited lanes) / alpha.
 // Levels come out per root in original-id order through a shared-memory
 // transpose; the whole launch sequence is captured once as a CUDA graph and
 // replayed for every batch.
@@ -52,13 +55,15 @@ struct MsParams {
   const uint32_t* __restrict__ col;
   const uint32_t* __restrict__ reorder;
   uint32_t* V;
-  uint32_t* F;
+  uint32_t* F[2];            // frontier masks by level parity: level l reads F[(l - 1) & 1], writes F[l & 1]
   uint32_t* N;
   uint8_t* L;                // [nlv][W] levels, 255 unreached
   const int64_t* roots;      // [nroots] original ids (device)
   const int* nroots_dev;     // number of roots of this launch (device, set with the roots)
   const uint2* hub_tab;      // pull: [nhub_chunks] (hub row, chunk index within the row)
   int64_t nhub_chunks;
+  const uint32_t* hubs;      // pull: the hub rows themselves
+  int64_t nhubs;
   const uint2* push_tab;     // push: [npush_chunks] the same for rows over MS_PUSH_HUB_DEG
   int64_t npush_chunks;
   int64_t nlv;
@@ -139,17 +144,95 @@ constexpr int MS_PUSH_HUB_DEG = 256;   // push: the same two, smaller: a push wa
 constexpr int MS_PUSH_CHUNK = 256;     //   frontier rows, so short chunks spread the few hub rows wider
 
 
+// byte mask of the 4 lanes whose bits are set in nib (bit i -> byte i)
+__device__ __forceinline__ uint32_t nibble_bytes(uint32_t nib) {
+  return ((nib * 0x00204081u) & 0x01010101u) * 0xFFu;
+}
+
+// level bytes of a row: for each 16-lane group with new lanes, write the
+// group's 16 bytes (new lanes = level, unvisited lanes = 255, lanes visited
+// before keep their byte, read back only when the group has such lanes).
+// Groups without visited lanes are never written; the output pass reads
+// them as 255 from the visited mask.
+template <int NW>
+__device__ __forceinline__ void write_levels(uint8_t* row, const Mask<NW>& nw, const Mask<NW>& vv, uint32_t lvl4) {
+#pragma unroll
+  for (int g = 0; g < 2 * NW; ++g) {
+    const uint32_t bits = (nw.w[g >> 1] >> ((g & 1) * 16)) & 0xFFFFu;
+    if (!bits) continue;
+    const uint32_t old = (vv.w[g >> 1] >> ((g & 1) * 16)) & 0xFFFFu;
+    uint4* dst = reinterpret_cast<uint4*>(row) + g;
+    uint4 o = make_uint4(~0u, ~0u, ~0u, ~0u);
+    if (old) o = __ldcg(dst);
+    uint32_t w[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint32_t bm = nibble_bytes((bits >> (4 * i)) & 0xFu);
+      w[i] = (w[i] & ~bm) | (lvl4 & bm);
+    }
+    *dst = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+// Per-thread counters of a level, flushed once per block at its end.
+template <int NW>
+struct LevelAcc {
+  unsigned long long nnew, nf, mf, mu;
+  Mask<NW> lanes;  // lanes that found vertices
+  __device__ void clear() {
+    nnew = nf = mf = mu = 0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) lanes.w[k] = 0;
+  }
+};
+
+// Vertex v (visited lanes vv, still-needed lanes need) found lanes nw this
+// level: its next-frontier mask (always written: the buffer holds an older
+// level), visited mask, level bytes and the counters of the direction rule.
+template <int NW>
+__device__ __forceinline__ void settle(const MsParams& p, uint32_t* Fn, int64_t v, const Mask<NW>& vv,
+                                       const Mask<NW>& need, const Mask<NW>& nw, uint32_t deg, uint32_t lvl4,
+                                       LevelAcc<NW>& a) {
+  constexpr int W = 32 * NW;
+  store_mask<NW>(Fn + v * NW, nw);
+  bool anynew = false, left = false;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) {
+    anynew |= nw.w[k] != 0;
+    left |= (need.w[k] & ~nw.w[k]) != 0;
+  }
+  if (anynew) {
+    Mask<NW> vn;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) vn.w[k] = vv.w[k] | nw.w[k];
+    store_mask<NW>(p.V + v * NW, vn);
+    write_levels<NW>(p.L + v * W, nw, vv, lvl4);
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      a.lanes.w[k] |= nw.w[k];
+      a.nnew += __popc(nw.w[k]);
+    }
+    ++a.nf;
+    a.mf += deg;
+  }
+  if (left) a.mu += deg;  // still has unvisited live lanes after this level
+}
+
 // pull over non-hub rows.  A row of at most MS_SMALL_DEG edges is walked by
 // its own thread, MS_UNROLL neighbours per step; a longer one by the whole
 // warp, 32 * MS_UNROLL neighbours per step (rows taken in turn).  Either stops
 // once the row's unvisited lanes are all found; under VERTEX_REORDERING=2 a
 // row lists its highest-degree neighbours first, which find most of them.
+// Each row is its own only writer, so it settles at once (next frontier,
+// visited mask, levels): pull levels need no separate apply pass over all
+// vertices, only one over the hub rows.
 template <int NW>
-__device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act) {
+__device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, const uint32_t* Fc, uint32_t* Fn,
+                             uint32_t lvl4, LevelAcc<NW>& la) {
   const int lane = threadIdx.x & 31;
   for (int64_t base = gwarp_id() * 32; base < p.nlv; base += gwarp_count() * 32) {
     const int64_t v = base + lane;
-    Mask<NW> need, acc;
+    Mask<NW> need, acc, vv;
     bool any = false;
     uint32_t deg = 0;
     uint64_t rb = 0;
@@ -157,9 +240,10 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act) {
     for (int k = 0; k < NW; ++k) {
       acc.w[k] = 0;
       need.w[k] = 0;
+      vv.w[k] = 0;
     }
     if (v < p.nlv) {
-      const Mask<NW> vv = load_mask<NW>(p.V + v * NW);
+      vv = load_mask<NW>(p.V + v * NW);
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
         need.w[k] = act.w[k] & ~vv.w[k];
@@ -179,7 +263,7 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act) {
 #pragma unroll
         for (int t = 0; t < MS_UNROLL; ++t)
           if (nb[t] != NO_VERTEX) {
-            const Mask<NW> f = gather_mask<NW>(p.F + (int64_t)nb[t] * NW);
+            const Mask<NW> f = gather_mask<NW>(Fc + (int64_t)nb[t] * NW);
 #pragma unroll
             for (int q = 0; q < NW; ++q) acc.w[q] |= f.w[q];
           }
@@ -211,7 +295,7 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act) {
 #pragma unroll
         for (int t = 0; t < MS_UNROLL; ++t)
           if (nb[t] != NO_VERTEX) {
-            const Mask<NW> f = gather_mask<NW>(p.F + (int64_t)nb[t] * NW);
+            const Mask<NW> f = gather_mask<NW>(Fc + (int64_t)nb[t] * NW);
 #pragma unroll
             for (int q = 0; q < NW; ++q) x.w[q] |= f.w[q];
           }
@@ -221,15 +305,12 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act) {
       }
       if (lane == src) acc = a;
     }
-    if (any && deg <= (uint32_t)MS_HUB_DEG) {
-      Mask<NW> out;
-      bool found = false;
+    // hub rows settle after the hub phase (deg is 0 here for rows without needed lanes)
+    if (v < p.nlv && deg <= (uint32_t)MS_HUB_DEG) {
+      Mask<NW> nw;
 #pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        out.w[k] = acc.w[k] & need.w[k];
-        found |= out.w[k] != 0;
-      }
-      if (found) store_mask<NW>(p.N + v * NW, out);  // N is zero outside the rows that found lanes
+      for (int k = 0; k < NW; ++k) nw.w[k] = acc.w[k] & need.w[k];
+      settle<NW>(p, Fn, v, vv, need, nw, deg, lvl4, la);
     }
   }
 }
@@ -252,7 +333,7 @@ __device__ __forceinline__ void hub_bounds(const MsParams& p, uint32_t h, uint32
 // pull over hub rows: each chunk ORs its neighbours' frontier masks, stopping
 // once the row's unvisited lanes are covered, into the row's next mask
 template <int NW>
-__device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act) {
+__device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act, const uint32_t* Fc) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = gwarp_count();
   for (int64_t c0 = gwarp_id(); c0 < p.nhub_chunks; c0 += 32 * nwarps) {
@@ -298,7 +379,7 @@ __device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act) {
 #pragma unroll
         for (int t = 0; t < MS_UNROLL; ++t)
           if (nb[t] != NO_VERTEX) {
-            const Mask<NW> f = gather_mask<NW>(p.F + (int64_t)nb[t] * NW);
+            const Mask<NW> f = gather_mask<NW>(Fc + (int64_t)nb[t] * NW);
 #pragma unroll
             for (int q = 0; q < NW; ++q) x.w[q] |= f.w[q];
           }
@@ -320,7 +401,7 @@ __device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act) {
 // push from hub frontier rows: every neighbour of the chunk gets the lanes it
 // still lacks
 template <int NW>
-__device__ void ms_push_hubs(const MsParams& p) {
+__device__ void ms_push_hubs(const MsParams& p, const uint32_t* Fc) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = gwarp_count();
   for (int64_t c0 = gwarp_id(); c0 < p.npush_chunks; c0 += 32 * nwarps) {
@@ -332,7 +413,7 @@ __device__ void ms_push_hubs(const MsParams& p) {
     for (int k = 0; k < NW; ++k) f.w[k] = 0;
     if (c < p.npush_chunks) {
       hd = __ldg(p.push_tab + c);
-      f = load_mask<NW>(p.F + (int64_t)hd.x * NW);
+      f = load_mask<NW>(Fc + (int64_t)hd.x * NW);
 #pragma unroll
       for (int k = 0; k < NW; ++k) any |= f.w[k] != 0;
     }
@@ -374,14 +455,14 @@ __device__ void ms_push_hubs(const MsParams& p) {
 // edges walked as one list, MS_WIN at a time; every neighbour gets the lanes
 // it still lacks.
 template <int NW>
-__device__ void ms_push_rows(const MsParams& p) {
+__device__ void ms_push_rows(const MsParams& p, const uint32_t* Fc) {
   const int lane = threadIdx.x & 31;
   for (int64_t base = gwarp_id() * (32 * MS_GROUPS); base < p.nlv; base += gwarp_count() * (32 * MS_GROUPS)) {
     Mask<NW> fg[MS_GROUPS];
 #pragma unroll
     for (int g = 0; g < MS_GROUPS; ++g) {
       const int64_t v = base + g * 32 + lane;
-      if (v < p.nlv) fg[g] = load_mask<NW>(p.F + v * NW);
+      if (v < p.nlv) fg[g] = load_mask<NW>(Fc + v * NW);
       else
 #pragma unroll
         for (int k = 0; k < NW; ++k) fg[g].w[k] = 0;
@@ -431,53 +512,16 @@ __device__ void ms_push_rows(const MsParams& p) {
   }
 }
 
-// byte mask of the 4 lanes whose bits are set in nib (bit i -> byte i)
-__device__ __forceinline__ uint32_t nibble_bytes(uint32_t nib) {
-  return ((nib * 0x00204081u) & 0x01010101u) * 0xFFu;
-}
-
-// level bytes of a row: for each 16-lane group with new lanes, write the
-// group's 16 bytes (new lanes = level, unvisited lanes = 255, lanes visited
-// before keep their byte, read back only when the group has such lanes).
-// Groups without visited lanes are never written; the output pass reads
-// them as 255 from the visited mask.
+// apply after a push level: new = N & needed lanes; settle every vertex (its
+// next-frontier mask is always written).  U vertices per thread per step,
+// loads first.
 template <int NW>
-__device__ __forceinline__ void write_levels(uint8_t* row, const Mask<NW>& nw, const Mask<NW>& vv, uint32_t lvl4) {
-#pragma unroll
-  for (int g = 0; g < 2 * NW; ++g) {
-    const uint32_t bits = (nw.w[g >> 1] >> ((g & 1) * 16)) & 0xFFFFu;
-    if (!bits) continue;
-    const uint32_t old = (vv.w[g >> 1] >> ((g & 1) * 16)) & 0xFFFFu;
-    uint4* dst = reinterpret_cast<uint4*>(row) + g;
-    uint4 o = make_uint4(~0u, ~0u, ~0u, ~0u);
-    if (old) o = __ldcg(dst);
-    uint32_t w[4] = {o.x, o.y, o.z, o.w};
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const uint32_t bm = nibble_bytes((bits >> (4 * i)) & 0xFu);
-      w[i] = (w[i] & ~bm) | (lvl4 & bm);
-    }
-    *dst = make_uint4(w[0], w[1], w[2], w[3]);
-  }
-}
-
-// apply: new = N & ~V; V |= new; F = new; N = 0; level bytes; counters for the
-// next direction decision.  MS_APPLY_U vertices per thread per step, loads
-// first; only words that change are stored.
-template <int NW>
-__device__ void ms_apply(const MsParams& p, const Mask<NW>& act, int level, unsigned long long* sh_acc,
-                         unsigned* sh_or, unsigned* alive_out) {
-  constexpr int W = 32 * NW;
+__device__ void ms_apply(const MsParams& p, const Mask<NW>& act, uint32_t* Fn, uint32_t lvl4, LevelAcc<NW>& la) {
   constexpr int U = NW == 4 ? 2 : 4;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
-  const uint32_t lvl4 = (uint32_t)level * 0x01010101u;
-  unsigned long long nnew = 0, nf = 0, mf = 0, mu = 0;
-  Mask<NW> lanes_new;
-#pragma unroll
-  for (int k = 0; k < NW; ++k) lanes_new.w[k] = 0;
   for (int64_t v0 = tid; v0 < p.nlv; v0 += nthreads * U) {
-    Mask<NW> n[U], vv[U], f[U];
+    Mask<NW> n[U], vv[U];
     uint32_t dg[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -485,60 +529,76 @@ __device__ void ms_apply(const MsParams& p, const Mask<NW>& act, int level, unsi
       if (v < p.nlv) {
         n[u] = load_mask<NW>(p.N + v * NW);
         vv[u] = load_mask<NW>(p.V + v * NW);
-        f[u] = load_mask<NW>(p.F + v * NW);
         dg[u] = __ldg(p.deg + v);
       } else {
         dg[u] = 0;
 #pragma unroll
-        for (int k = 0; k < NW; ++k) n[u].w[k] = vv[u].w[k] = f[u].w[k] = 0;
+        for (int k = 0; k < NW; ++k) n[u].w[k] = vv[u].w[k] = 0;
       }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t v = v0 + u * nthreads;
-      Mask<NW> nw, vnew;
-      bool anyn = false, anynew = false, fchg = false, done = true;
+      if (v >= p.nlv) continue;
+      Mask<NW> need, nw;
+      bool anyn = false;
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
-        nw.w[k] = n[u].w[k] & ~vv[u].w[k];
-        vnew.w[k] = vv[u].w[k] | nw.w[k];
+        need.w[k] = act.w[k] & ~vv[u].w[k];
+        nw.w[k] = n[u].w[k] & need.w[k];
         anyn |= n[u].w[k] != 0;
-        anynew |= nw.w[k] != 0;
-        fchg |= f[u].w[k] != nw.w[k];
-        done &= (vnew.w[k] & act.w[k]) == act.w[k];
       }
-      if (v >= p.nlv) continue;
       if (anyn) {
         Mask<NW> zero;
 #pragma unroll
         for (int k = 0; k < NW; ++k) zero.w[k] = 0;
         store_mask<NW>(p.N + v * NW, zero);
       }
-      if (fchg) store_mask<NW>(p.F + v * NW, nw);
-      if (anynew) {
-        store_mask<NW>(p.V + v * NW, vnew);
-        write_levels<NW>(p.L + v * W, nw, vv[u], lvl4);
-#pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          lanes_new.w[k] |= nw.w[k];
-          nnew += __popc(nw.w[k]);
-        }
-      }
-      if (anynew) {
-        ++nf;
-        mf += dg[u];
-      }
-      if (!done) mu += dg[u];
+      settle<NW>(p, Fn, v, vv[u], need, nw, dg[u], lvl4, la);
     }
   }
-  block_add(sh_acc, M_NEW, nnew);
-  block_add(sh_acc, M_NF, nf);
-  block_add(sh_acc, M_MF, mf);
-  block_add(sh_acc, M_MU, mu);
-  // lanes that found vertices stay alive; the others have finished their BFS
+}
+
+// after a pull level: the hub rows, whose chunks ORed into N
+template <int NW>
+__device__ void ms_settle_hubs(const MsParams& p, const Mask<NW>& act, uint32_t* Fn, uint32_t lvl4,
+                               LevelAcc<NW>& la) {
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = tid; i < p.nhubs; i += nthreads) {
+    const uint32_t h = __ldg(p.hubs + i);
+    const Mask<NW> n = load_mask<NW>(p.N + (int64_t)h * NW);
+    const Mask<NW> vv = load_mask<NW>(p.V + (int64_t)h * NW);
+    Mask<NW> need, nw;
+    bool anyn = false;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      need.w[k] = act.w[k] & ~vv.w[k];
+      nw.w[k] = n.w[k] & need.w[k];
+      anyn |= n.w[k] != 0;
+    }
+    if (anyn) {
+      Mask<NW> zero;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) zero.w[k] = 0;
+      store_mask<NW>(p.N + (int64_t)h * NW, zero);
+    }
+    settle<NW>(p, Fn, h, vv, need, nw, __ldg(p.deg + h), lvl4, la);
+  }
+}
+
+// the level's counters into the block accumulators, and the lanes that found
+// vertices (the others have finished their BFS) into alive_out
+template <int NW>
+__device__ void flush_level(const LevelAcc<NW>& la, unsigned long long* sh_acc, unsigned* sh_or,
+                            unsigned* alive_out) {
+  block_add(sh_acc, M_NEW, la.nnew);
+  block_add(sh_acc, M_NF, la.nf);
+  block_add(sh_acc, M_MF, la.mf);
+  block_add(sh_acc, M_MU, la.mu);
 #pragma unroll
   for (int k = 0; k < NW; ++k) {
-    const unsigned x = __reduce_or_sync(FULL_MASK, lanes_new.w[k]);
+    const unsigned x = __reduce_or_sync(FULL_MASK, la.lanes.w[k]);
     if ((threadIdx.x & 31) == 0 && x) atomicOr(&sh_or[k], x);
   }
   __syncthreads();
@@ -570,9 +630,9 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
     Mask<NW> zero;
 #pragma unroll
     for (int k = 0; k < NW; ++k) zero.w[k] = 0;
-    for (int64_t v = tid; v < p.nlv; v += nthreads) {
+    for (int64_t v = tid; v < p.nlv; v += nthreads) {  // F[1] is written whole by level 1
       store_mask<NW>(p.V + v * NW, zero);
-      store_mask<NW>(p.F + v * NW, zero);
+      store_mask<NW>(p.F[0] + v * NW, zero);
       store_mask<NW>(p.N + v * NW, zero);
     }
   }
@@ -587,7 +647,7 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
     const uint32_t r = __ldg(p.reorder + p.roots[tid]);
     if ((int64_t)r < p.nlv) {
       atomicOr(p.V + (int64_t)r * NW + tid / 32, 1u << (tid & 31));
-      atomicOr(p.F + (int64_t)r * NW + tid / 32, 1u << (tid & 31));
+      atomicOr(p.F[0] + (int64_t)r * NW + tid / 32, 1u << (tid & 31));
       p.L[(int64_t)r * W + tid] = 0;
       mf0 = __ldg(p.off + r + 1) - __ldg(p.off + r);
     }
@@ -604,17 +664,24 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
     unsigned* alive = ctl->alive[phase % 3];
     if (blockIdx.x == 0 && threadIdx.x < M_NUM) ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0;
     if (blockIdx.x == 0 && threadIdx.x < 4) ctl->alive[(phase + 1) % 3][threadIdx.x] = 0;
+    const uint32_t* Fc = p.F[(level - 1) & 1];
+    uint32_t* Fn = p.F[level & 1];
+    const uint32_t lvl4 = (uint32_t)level * 0x01010101u;
+    LevelAcc<NW> la;
+    la.clear();
     if (pull) {
-      ms_pull_rows<NW>(p, act);
-      ms_pull_hubs<NW>(p, act);
+      ms_pull_rows<NW>(p, act, Fc, Fn, lvl4, la);
+      ms_pull_hubs<NW>(p, act, Fc);
     } else {
-      ms_push_rows<NW>(p);
-      ms_push_hubs<NW>(p);
+      ms_push_rows<NW>(p, Fc);
+      ms_push_hubs<NW>(p, Fc);
     }
     pulls += pull;
     if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
     if (tid == 0) ctl->level_mid_ns[level] = globaltimer();
-    ms_apply<NW>(p, act, level, sh_acc, sh_or, alive);
+    if (pull) ms_settle_hubs<NW>(p, act, Fn, lvl4, la);
+    else ms_apply<NW>(p, act, Fn, lvl4, la);
+    flush_level<NW>(la, sh_acc, sh_or, alive);
     if (!grid_sync<M_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
     ++phase;
     const unsigned long long nnew = sh_cnt[M_NEW];
@@ -834,6 +901,8 @@ struct g500_msbfs {
   uint32_t* deg = nullptr;                            // [nlv] row lengths
   uint2* hub_tab = nullptr;                           // pull: [nhub_chunks] (hub row, chunk index)
   int64_t nhub_chunks = 0;
+  uint32_t* hub_rows = nullptr;                       // pull: the rows longer than MS_HUB_DEG
+  int64_t nhub_rows = 0;
   uint2* push_tab = nullptr;                          // push: [npush_chunks]
   int64_t npush_chunks = 0;
   int last_nroots = 0;
@@ -867,6 +936,7 @@ static int ms_free(g500_msbfs* m) {
   dev_free(m->stats_dev);
   dev_free(m->deg);
   dev_free(m->hub_tab);
+  dev_free(m->hub_rows);
   dev_free(m->push_tab);
   if (m->staging) cudaFreeHost(m->staging);
   if (m->h_ctl) cudaFreeHost(m->h_ctl);
@@ -884,7 +954,8 @@ static const void* ms_kernel_ptr() { return (const void*)msbfs_kernel<NW>; }
 
 // Chunk table of the rows longer than `thresh`, `chunk` edges per chunk, so
 // that warps can share a hub's row.
-static int ms_build_hubs(g500_msbfs* m, uint64_t thresh, uint64_t chunk, uint2** tab, int64_t* ntab) {
+static int ms_build_hubs(g500_msbfs* m, uint64_t thresh, uint64_t chunk, uint2** tab, int64_t* ntab,
+                         uint32_t** rows_out = nullptr, int64_t* nrows_out = nullptr) {
   g500_graph* g = m->g;
   cudaStream_t s = m->stream;
   const int64_t nlv = g->nlv;
@@ -932,7 +1003,12 @@ static int ms_build_hubs(g500_msbfs* m, uint64_t thresh, uint64_t chunk, uint2**
     }
   }
   dev_free(flags);
-  dev_free(hubs);
+  if (rows_out && st == G500_OK) {
+    *rows_out = hubs;  // the handle keeps the hub rows
+    *nrows_out = (int64_t)H;
+  } else {
+    dev_free(hubs);
+  }
   dev_free(pos);
   dev_free(chunks);
   dev_free(chunk0);
@@ -957,7 +1033,10 @@ static int ms_enqueue_batch(g500_msbfs* m, int b, cudaStream_t s) {
   p.col = g->d_cols;
   p.reorder = g->d_reorder;
   p.V = m->V;
-  p.F = m->F;
+  p.F[0] = m->F;
+  p.F[1] = m->F + std::max<int64_t>(g->nlv, 1) * 4;
+  p.hubs = m->hub_rows;
+  p.nhubs = m->nhub_rows;
   p.N = m->N;
   p.L = m->L;
   p.roots = m->roots_dev + b * MS_MAX_LANES;
@@ -1003,7 +1082,7 @@ extern "C" int g500_msbfs_create(g500_graph* g, g500_msbfs** out) {
   chk(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking), "cudaStreamCreate");
   const int64_t nlv = std::max<int64_t>(g->nlv, 1);
   if (st == G500_OK) st = dev_alloc_n(&m->V, nlv * 4, "msbfs visited masks");
-  if (st == G500_OK) st = dev_alloc_n(&m->F, nlv * 4, "msbfs frontier masks");
+  if (st == G500_OK) st = dev_alloc_n(&m->F, 2 * nlv * 4, "msbfs frontier masks");
   if (st == G500_OK) st = dev_alloc_n(&m->N, nlv * 4, "msbfs next masks");
   if (st == G500_OK) st = dev_alloc_n(&m->L, nlv * MS_MAX_LANES, "msbfs levels");
   if (st == G500_OK) st = dev_alloc_n(&m->deg, nlv, "msbfs row lengths");
@@ -1026,7 +1105,8 @@ extern "C" int g500_msbfs_create(g500_graph* g, g500_msbfs** out) {
   if (st == G500_OK)
     chk(cudaHostAlloc(&m->h_stats, sizeof(unsigned long long) * 2 * MS_MAX_LANES, cudaHostAllocDefault),
         "cudaHostAlloc");
-  if (st == G500_OK) st = ms_build_hubs(m, MS_HUB_DEG, MS_HUB_CHUNK, &m->hub_tab, &m->nhub_chunks);
+  if (st == G500_OK)
+    st = ms_build_hubs(m, MS_HUB_DEG, MS_HUB_CHUNK, &m->hub_tab, &m->nhub_chunks, &m->hub_rows, &m->nhub_rows);
   if (st == G500_OK) st = ms_build_hubs(m, MS_PUSH_HUB_DEG, MS_PUSH_CHUNK, &m->push_tab, &m->npush_chunks);
   const void* kernels[3] = {ms_kernel_ptr<1>(), ms_kernel_ptr<2>(), ms_kernel_ptr<4>()};
   for (int i = 0; i < 3 && st == G500_OK; ++i) {
@@ -1250,7 +1330,7 @@ extern "C" int g500_msbfs_workspace_bytes(const g500_graph* g, uint64_t* bytes) 
   const uint64_t nlv = (uint64_t)std::max<int64_t>(g->nlv, 1);
   // V, F, N (4 words each), L (128 bytes), row lengths, output rows, with room
   // for the hub tables and control blocks
-  *bytes = nlv * (3 * 16 + MS_MAX_LANES + 4) + (uint64_t)MS_MAX_LANES * (uint64_t)g->nolv + (16ull << 20) +
+  *bytes = nlv * (4 * 16 + MS_MAX_LANES + 4) + (uint64_t)MS_MAX_LANES * (uint64_t)g->nolv + (16ull << 20) +
            (uint64_t)g->nge / 64;
   return G500_OK;
 }
