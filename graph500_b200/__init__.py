@@ -155,6 +155,7 @@ def lib() -> C.CDLL:
         "g500_bfs_create": ([P, C.POINTER(P)], i32),
         "g500_bfs_set_params": ([P, C.c_double, C.c_double, i32], i32),
         "g500_bfs_set_stream": ([P, P], i32),
+        "g500_bfs_set_pred_mode": ([P, i32], i32),
         "g500_bfs_set_policy": ([P, i32], i32),
         "g500_bfs_autotune": ([P, P, i32, i32, C.POINTER(TuneResult)], i32),
         "g500_bfs_run": ([P, i64, P, i32, C.POINTER(BfsStats)], i32),
@@ -406,6 +407,10 @@ class BfsOnGPU:
         check(lib().g500_bfs_set_params(self.h, alpha, beta, int(count_edges)))
         if policy is not None:
             check(lib().g500_bfs_set_policy(self.h, policy))
+
+    def set_pred_mode(self, mode: int = 0) -> None:
+        """0 by pred size, 1 pred written as vertices are found, 2 deferred (one pass at the end)."""
+        check(lib().g500_bfs_set_pred_mode(self.h, mode))
 
     def autotune(self, roots, reps: int = 2) -> dict:
         """Pick the direction policy and thresholds on sample roots (kept on the handle)."""

@@ -11,7 +11,10 @@
 //   queue[2]  top-down work items (vertex, chunk): a row is cut into chunks of
 //             TD_CHUNK edges so a hub spreads over many warps
 //   pred      int64 per ORIGINAL id: parent | level << 48 (bfs.hpp:1203,
-//             :2470), root = root (:498), -1 unreached
+//             :2470), root = root (:498), -1 unreached.  Written as vertices
+//             are found, or (deferred mode, for pred arrays beyond L2) by
+//             reordered id into pred_r during the search and in original-id
+//             order by one sequential pass at the end
 //
 // Top-down (top_down_search, bfs.hpp:1139-1166, :1249-1364): a warp takes B
 // work items (B adapts to the queue length so every warp has work), prefix-
@@ -39,6 +42,12 @@
 namespace g500 {
 
 constexpr int BFS_THREADS = 512;
+// pred arrays larger than this (beyond what L2 keeps) are written in deferred
+// mode: the search records pred entries by reordered id, contiguous and
+// coalesced, and one final pass writes pred in original-id order; writing
+// pred at random during the search costs a DRAM read-modify-write per
+// discovered vertex once pred no longer fits in L2.
+constexpr uint64_t BFS_DEFERRED_PRED_BYTES = 64ull << 20;
 constexpr int BFS_MIN_BLOCKS = 2;        // co-resident blocks per SM (64 registers, no spills)
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
 constexpr int BU_WORDS = 8;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
@@ -52,6 +61,8 @@ struct RunParams {
   const uint32_t* __restrict__ reorder;
   const uint32_t* __restrict__ vis_init;
   int64_t* __restrict__ pred;
+  int64_t* __restrict__ pred_r;  // deferred mode: pred entries by reordered id, [nlv]
+  int deferred;                  // write pred_r during the search, pred in one pass at the end
   uint32_t* vis[2];
   TdItem* queue[2];
   BfsCtl* ctl;
@@ -167,7 +178,8 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
         ow[j] = 0;
         if (won[j]) {
           ow[j] = __ldg(p.invert + w[j]);
-          p.pred[ow[j]] = (int64_t)uo[j] | lvl;
+          if (p.deferred) p.pred_r[w[j]] = (int64_t)uo[j] | lvl;
+          else p.pred[ow[j]] = (int64_t)uo[j] | lvl;
           if (p.policy == G500_DIR_EDGES) mf += __ldg(p.off + w[j] + 1) - __ldg(p.off + w[j]);
         }
       }
@@ -260,7 +272,12 @@ __device__ void bu_pass_a(const RunParams& p, const uint32_t* __restrict__ vis_c
           scanned += __popc(~wv[u]);
           nmiss += __popc(misses);
         }
-        if (hit) p.pred[__ldg(p.invert + (wbase + js[u]) * 32 + lane)] = (int64_t)__ldg(p.invert + pf[u]) | lvl;
+        if (hit) {
+          const int64_t vr = (wbase + js[u]) * 32 + lane;
+          const int64_t val = (int64_t)__ldg(p.invert + pf[u]) | lvl;
+          if (p.deferred) p.pred_r[vr] = val;
+          else p.pred[__ldg(p.invert + vr)] = val;
+        }
       }
     }
   }
@@ -340,7 +357,9 @@ __device__ void bu_pass_b(const RunParams& p, const uint32_t* __restrict__ vis_c
       }
       if (parent != NO_VERTEX) {
         atomicOr(vis_next + (v >> 5), 1u << (v & 31));
-        p.pred[__ldg(p.invert + v)] = (int64_t)__ldg(p.invert + parent) | lvl;
+        const int64_t val = (int64_t)__ldg(p.invert + parent) | lvl;
+        if (p.deferred) p.pred_r[v] = val;
+        else p.pred[__ldg(p.invert + v)] = val;
         ++found;
       }
       if (p.count_edges && v != NO_VERTEX) {
@@ -415,9 +434,11 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   uint2* found_list = reinterpret_cast<uint2*>(p.queue[1]);
   if (threadIdx.x < C_NUM) sh_acc[threadIdx.x] = 0;
 
-  // initialize_memory (bfs.hpp:241-276): pred = -1, visited = ~has_edge
+  // initialize_memory (bfs.hpp:241-276): pred = -1, visited = ~has_edge.  In
+  // deferred mode pred is written whole by the final pass instead.
   if (tid == 0) ctl->t0_ns = globaltimer();
-  for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = -1;
+  if (!p.deferred)
+    for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = -1;
   for (int64_t i = tid; i < p.nwords; i += nthreads) p.vis[0][i] = p.vis_init[i];
   if (blockIdx.x == 0 && threadIdx.x < 3 * C_NUM) (&ctl->cnt[0][0])[threadIdx.x] = 0;
   const uint32_t root_r = p.reorder[p.root];
@@ -437,11 +458,14 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
     items[c] = it;
   }
   if (tid == 0) {
-    p.pred[p.root] = p.root;
+    if (!p.deferred) p.pred[p.root] = p.root;
+    else if (has_edges) p.pred_r[root_r] = p.root;
     if (has_edges) p.vis[0][root_r >> 5] |= 1u << (root_r & 31);
     ctl->root_has_edges = has_edges ? 1 : 0;
   }
   if (!has_edges) {
+    if (p.deferred)  // the search is over before it starts: only the root has a parent
+      for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = i == p.root ? p.root : -1;
     if (tid == 0) {
       ctl->num_levels = 0;
       ctl->final_vis = 0;
@@ -547,6 +571,20 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
                    edges + (was_forward ? carried_in : 0), sect + (was_forward ? carried_in : 0), t_mid);
   }
 #undef NEXT_PHASE_SLOT
+  if (p.deferred) {
+    // pred in original-id order, sequential writes: a reached vertex (visited
+    // now, not pre-visited for lack of edges) takes its entry from pred_r
+    const uint32_t* vf = p.vis[cur_vis];
+    for (int64_t u = tid; u < p.nolv; u += nthreads) {
+      const uint32_t r = __ldg(p.reorder + u);
+      int64_t val = -1;
+      if ((int64_t)r < p.nlv) {
+        const uint32_t bit = 1u << (r & 31);
+        if ((__ldcg(vf + (r >> 5)) & ~__ldg(p.vis_init + (r >> 5))) & bit) val = __ldcg(p.pred_r + r);
+      }
+      p.pred[u] = val;
+    }
+  }
   if (tid == 0) {
     ctl->num_levels = (unsigned)level;
     ctl->final_vis = cur_vis;
@@ -586,6 +624,7 @@ static int bfs_free(g500_bfs* b) {
   cudaSetDevice(b->g->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   dev_free(b->d_pred);
+  dev_free(b->d_pred_r);
   dev_free(b->d_vis[0]);
   dev_free(b->d_vis[1]);
   dev_free(b->d_queue[0]);
@@ -649,6 +688,13 @@ extern "C" int g500_bfs_set_params(g500_bfs* b, double alpha, double beta, int c
   b->alpha = alpha;
   b->beta = beta;
   b->count_edges = count_edges ? 1 : 0;
+  return G500_OK;
+}
+
+extern "C" int g500_bfs_set_pred_mode(g500_bfs* b, int mode) {
+  if (!b) return set_error(G500_E_INVAL, "null bfs");
+  if (mode < 0 || mode > 2) return set_error(G500_E_INVAL, "unknown pred mode %d", mode);
+  b->pred_mode = mode;
   return G500_OK;
 }
 
@@ -739,6 +785,9 @@ extern "C" int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_o
   p.reorder = g->d_reorder;
   p.vis_init = g->d_vis_init;
   p.pred = pred_on_device ? pred : b->d_pred;
+  p.deferred = b->pred_mode == 2 || (b->pred_mode == 0 && (uint64_t)g->nolv * 8 > BFS_DEFERRED_PRED_BYTES);
+  if (p.deferred && !b->d_pred_r) G500_TRY(dev_alloc_n(&b->d_pred_r, std::max<int64_t>(g->nlv, 1), "deferred pred"));
+  p.pred_r = b->d_pred_r;
   p.vis[0] = b->d_vis[0];
   p.vis[1] = b->d_vis[1];
   p.queue[0] = b->d_queue[0];

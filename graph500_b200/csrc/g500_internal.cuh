@@ -166,6 +166,8 @@ struct g500_bfs {
   unsigned grid = 0;                 // co-resident blocks of the persistent kernel
 
   int64_t* d_pred = nullptr;         // [nolv]
+  int64_t* d_pred_r = nullptr;       // [nlv] deferred mode: pred entries by reordered id
+  int pred_mode = 0;                 // 0 by pred size, 1 direct, 2 deferred
   uint32_t* d_vis[2] = {nullptr, nullptr};
   TdItem* d_queue[2] = {nullptr, nullptr};
   int64_t queue_cap = 0;

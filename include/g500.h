@@ -157,6 +157,10 @@ enum g500_dir_policy { G500_DIR_REFERENCE = 0, G500_DIR_EDGES = 1 };
 int g500_bfs_set_policy(g500_bfs* b, int policy);
 /* Use this stream for the runs (NULL = the handle's own stream). */
 int g500_bfs_set_stream(g500_bfs* b, void* stream);
+/* How run writes pred: 0 (default) by its size, 1 at random as vertices are
+ * discovered, 2 deferred: entries by reordered id during the search, then one
+ * sequential pass in original-id order.  Results are identical. */
+int g500_bfs_set_pred_mode(g500_bfs* b, int mode);
 
 /* Autotuner: time every (policy, alpha, beta) of a built-in grid on the given
  * roots (device pred, best of `reps` runs per root), keep the fastest on the

@@ -84,12 +84,14 @@ def test_graph_info_and_roots_match_reference(g500, scale, vr):
 
 
 # ----------------------------------------------------------------------- BFS
+@pytest.mark.parametrize("pred_mode", [1, 2])  # pred written as found / deferred to one final pass
 @pytest.mark.parametrize("scale,vr", GOLDEN_CASES)
-def test_bfs_levels_and_validation(g500, oracle_mod, scale, vr):
+def test_bfs_levels_and_validation(g500, oracle_mod, scale, vr, pred_mode):
     rec, arr = load_golden(scale, vr)
     bfs = g500.BfsOnGPU(reorder_mode=vr)
     bfs.construct(g500.EdgeList(None, scale, 16))
     bfs.prepare_bfs()
+    bfs.set_pred_mode(pred_mode)
     edges = oracle_mod.generate_edges(scale) if scale <= 16 else None
     pred = np.zeros(bfs.graph_.pred_size(), np.int64)
     for i, pr in enumerate(rec["per_root"]):
@@ -195,9 +197,10 @@ def _edges_from_pairs(g500, pairs):
     return a
 
 
+@pytest.mark.parametrize("pred_mode", [1, 2])
 @pytest.mark.parametrize("name", ["path", "star", "two_components", "self_loops_dups", "high_ids", "isolated_root"])
 @pytest.mark.parametrize("vr", [0, 1, 2])
-def test_small_graphs(g500, oracle_mod, name, vr):
+def test_small_graphs(g500, oracle_mod, name, vr, pred_mode):
     rng = np.random.default_rng(7)
     if name == "path":
         n = 3000  # depth > 255 levels
@@ -227,6 +230,7 @@ def test_small_graphs(g500, oracle_mod, name, vr):
     assert [info.log_orig_global_verts, info.pred_size, info.num_local_verts, info.num_global_verts,
             info.num_global_edges, info.max_used_vertex] == list(og.info.values())
     bfs.prepare_bfs()
+    bfs.set_pred_mode(pred_mode)
     pred = np.full(bfs.graph_.pred_size(), 777, np.int64)
     st = bfs.run_bfs(root, pred)
     lv = g500.levels_from_pred(pred)
