@@ -1,6 +1,8 @@
 """Build recipe for libg500.so: every CUDA source under csrc/ compiled for
 sm_100a with nvcc and linked into one shared library next to this file.
 
+Also builds g500_main, the main.cc-style benchmark driver (driver/g500_main.cc).
+
 Usage: python -m graph500_b200.build [-v] [--force]
 """
 from __future__ import annotations
@@ -16,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libg500.so")
+DRIVER = os.path.join(HERE, "g500_main")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -36,7 +39,7 @@ def sources() -> list[str]:
 
 def headers() -> list[str]:
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    return hs + [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
+    return hs + [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith((".h", ".hpp"))]
 
 
 def _stale(target: str, deps: list[str]) -> bool:
@@ -80,6 +83,15 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if r.returncode:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link failed")
+    # the main.cc-style driver: host C++ over the C ABI, next to the library
+    drv = os.path.join(HERE, "driver", "g500_main.cc")
+    if force or _stale(DRIVER, [drv, LIB] + hdrs):
+        cmd = ["g++", "-O2", "-std=c++17", "-I" + INCLUDE, drv, "-o", DRIVER, "-L" + HERE, "-lg500",
+               "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+        if r.returncode:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("driver build failed")
     return LIB
 
 
