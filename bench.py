@@ -75,6 +75,38 @@ def workload(a) -> dict:
             "parallelism": f"replicas x{a.gpus}"}
 
 
+# --------------------------------------------------------------------------- replicas
+class Replicas:
+    """The multi-GPU plumbing: one process per GPU, each with its own graph
+    and roots (replicas; no collective on the data path).  Only the merge of
+    the measurements crosses ranks: times as the max over ranks, edge counts
+    as sums, so value = all ranks' edges / the slowest rank's time."""
+
+    def __init__(self, dist=None, device: str = "cuda"):
+        self.dist, self.device = dist, device
+
+    def barrier(self) -> None:
+        if self.dist:
+            self.dist.barrier()
+
+    def _reduce(self, x: float, op) -> float:
+        if not self.dist:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x: float) -> float:
+        return self._reduce(x, self.dist.ReduceOp.MAX if self.dist else None)
+
+    def sum(self, x: float) -> float:
+        return self._reduce(x, self.dist.ReduceOp.SUM if self.dist else None)
+
+    def gteps(self, edges_rank: float, seconds_rank: float) -> float:
+        return self.sum(edges_rank) / self.max(seconds_rank) / 1e9
+
+
 # --------------------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -366,23 +398,8 @@ def our_arm(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
-    def barrier():
-        if dist:
-            dist.barrier()
-
-    def reduce_max(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def reduce_sum(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t)
-        return float(t.item())
+    rep = Replicas(dist, "cuda")
+    barrier, reduce_max, reduce_sum = rep.barrier, rep.max, rep.sum
 
     bfs = g5.BfsOnGPU(device=local, reorder_mode=a.reorder)
     t0 = time.time()
