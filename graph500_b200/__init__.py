@@ -29,7 +29,8 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "g500.h")
 USERSEED1, USERSEED2 = 2, 3  # mpi/parameters.h:190-191
 EDGE_DTYPE = np.dtype([("v0_low", "<u4"), ("v1_low", "<u4"), ("high", "<u4")])
 
-G500_OK, G500_E_INVAL, G500_E_NOMEM, G500_E_DEVICE, G500_E_TIMEOUT, G500_E_RANGE, G500_E_STATE = range(7)
+(G500_OK, G500_E_INVAL, G500_E_NOMEM, G500_E_DEVICE, G500_E_TIMEOUT, G500_E_RANGE, G500_E_STATE,
+ G500_E_VALIDATION, G500_E_IO) = range(9)
 
 
 class G500Error(RuntimeError):
@@ -150,6 +151,8 @@ def lib() -> C.CDLL:
         "g500_graph_find_roots": ([P, i32, u64, u64, P, C.POINTER(i32)], i32),
         "g500_graph_edges": ([P, C.POINTER(P), C.POINTER(i64)], i32),
         "g500_graph_copy_csr": ([P, P, P, P], i32),
+        "g500_graph_save": ([P, C.c_char_p], i32),
+        "g500_graph_load": ([C.c_char_p, i32, C.POINTER(P)], i32),
         "g500_graph_timings": ([P, C.POINTER(C.c_double), C.POINTER(C.c_double)], i32),
         "g500_graph_destroy": ([P], i32),
         "g500_bfs_create": ([P, C.POINTER(P)], i32),
@@ -311,6 +314,17 @@ class Graph2DCSR:
                  seed1: int = USERSEED1, seed2: int = USERSEED2):
         h = C.c_void_p()
         check(lib().g500_graph_generate(scale, edgefactor, seed1, seed2, reorder_mode, device, C.byref(h)))
+        return cls(h.value)
+
+    def save(self, path: str) -> None:
+        """Write the constructed graph to a snapshot file (g500_graph_save)."""
+        check(lib().g500_graph_save(self.h, os.fsencode(path)))
+
+    @classmethod
+    def load(cls, path: str, device: int = 0):
+        """A graph read back from a snapshot file onto `device` (g500_graph_load)."""
+        h = C.c_void_p()
+        check(lib().g500_graph_load(os.fsencode(path), device, C.byref(h)))
         return cls(h.value)
 
     def pred_size(self) -> int:

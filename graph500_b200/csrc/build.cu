@@ -369,7 +369,7 @@ static int build_from_device_edges(g500_graph* g, const g500_packed_edge* d_edge
   return G500_OK;
 }
 
-static int new_graph(int device, int reorder_mode, g500_graph** out) {
+int new_graph(int device, int reorder_mode, g500_graph** out) {
   if (!out) return set_error(G500_E_INVAL, "null output handle");
   if (reorder_mode < 0 || reorder_mode > 2) return set_error(G500_E_INVAL, "reorder_mode %d not in 0..2", reorder_mode);
   G500_CUDA(cudaSetDevice(device));

@@ -103,7 +103,7 @@ struct g500_graph {
   uint32_t* d_reorder = nullptr;    // [nolv]  original -> reordered
   uint32_t* d_invert = nullptr;     // [nolv]  reordered -> original
   uint32_t* d_vis_init = nullptr;   // [nlv/32] ~has_edge in reordered space
-  uint32_t* d_endp = nullptr;       // [nlv]   input endpoint occurrences per reordered vertex
+  uint32_t* d_endp = nullptr;       // [nolv]  input endpoint occurrences per reordered vertex
   g500_packed_edge* d_edges = nullptr;  // resident input edge list (optional)
   int64_t num_edges = 0;
   bool owns_edges = false;
@@ -182,4 +182,10 @@ namespace g500 {
 // g500_msbfs_launch that also copies each root's level row (pred_size bytes)
 // to root_dsts[i] when it is not null, before the launch's completion event.
 int msbfs_launch_to(g500_msbfs* m, const int64_t* roots, int nroots, uint8_t* const* root_dsts);
+}  // namespace g500
+
+namespace g500 {
+// An empty graph handle on `device` with its own stream (build.cu).
+int new_graph(int device, int reorder_mode, g500_graph** out);
+int graph_destroy_internal(g500_graph* g);
 }  // namespace g500

@@ -33,7 +33,8 @@ enum g500_status {
   G500_E_TIMEOUT = 4,  /* a bounded device-side wait gave up */
   G500_E_RANGE = 5,    /* size beyond what the format or a fixed buffer holds */
   G500_E_STATE = 6,    /* call out of order (e.g. run before create) */
-  G500_E_VALIDATION = 7
+  G500_E_VALIDATION = 7,
+  G500_E_IO = 8        /* a file could not be read or written, or is not what it claims */
 };
 
 /* The reference's packed edge: 48-bit endpoints in 12 bytes
@@ -111,6 +112,14 @@ int g500_graph_edges(const g500_graph* g, const g500_packed_edge** dev_edges, in
  * reordered).  Any pointer may be NULL. */
 int g500_graph_copy_csr(const g500_graph* g, uint64_t* offsets, uint32_t* cols,
                         uint32_t* reorder_map);
+/* CSR snapshots: the constructed graph (CSR, maps, bitmaps and the kept edge
+ * list, if any) written to a file and read back onto `device`, so that a
+ * serving process loads resident graphs without regenerating them.  No
+ * counterpart in the reference (its TMPFILE spill holds only the edge list,
+ * graph_generator.hpp:67-83).  Errors: G500_E_IO for unreadable, truncated or
+ * foreign files. */
+int g500_graph_save(const g500_graph* g, const char* path);
+int g500_graph_load(const char* path, int device, g500_graph** out);
 /* Seconds spent on the device in generation and construction. */
 int g500_graph_timings(const g500_graph* g, double* generation_s, double* construction_s);
 int g500_graph_destroy(g500_graph* g);
