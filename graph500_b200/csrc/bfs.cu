@@ -231,22 +231,27 @@ __device__ __forceinline__ bool vis_test(const uint32_t* __restrict__ vis, uint3
   return (__ldg(vis + (v >> 5)) >> (v & 31)) & 1u;
 }
 
-// Bottom-up pass A: lane l owns vertex l of a 32-vertex word, BU_WORDS words
-// in flight per warp.  Each unvisited vertex tests its first (smallest
-// reordered id; under VERTEX_REORDERING=2 the highest-degree) neighbour -- the
-// reference's isolated first edge.  New bits come from one ballot per word
-// (no atomics); the vertices that missed are marked in a miss bitmap.
-__device__ void bu_pass_a(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* __restrict__ vis_next,
-                          uint32_t* __restrict__ miss, unsigned long long* sh_acc, int64_t lvl) {
+// Bottom-up level (bottom_up_search_bitmap, bfs.hpp:1839-2038), one warp per
+// 32 words of the visited bitmap at a time, both steps on the same words so
+// that no grid barrier separates them:
+//  A. lane l owns vertex l of a word, BU_WORDS words in flight; each unvisited
+//     vertex tests its first neighbour (the reference's isolated first edge;
+//     under VERTEX_REORDERING=2 its highest-degree neighbour) against the
+//     visited map of the previous levels.  Hits come from one ballot per word
+//     and are written without atomics; the word's misses stay in a register of
+//     the lane that owns the word.
+//  B. the warp gathers 32 misses of its words into its lanes (select_bit); a
+//     lane checks BU_SERIAL more row entries alone, and rows still unresolved
+//     are scanned by the whole warp.
+__device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* __restrict__ vis_next,
+                         unsigned long long* sh_acc, int64_t lvl) {
   const int lane = threadIdx.x & 31;
-  unsigned long long found = 0, scanned = 0, nmiss = 0;
+  unsigned long long found_a = 0, found_b = 0, scanned = 0, edges = 0, sectors = 0;
   for (int64_t wbase = gwarp_id() * 32; wbase < p.nwords; wbase += gwarp_count() * 32) {
     const int64_t wi = wbase + lane;
     const uint32_t vw = wi < p.nwords ? __ldg(vis_cur + wi) : ~0u;
-    if (wi < p.nwords && vw == ~0u) {
-      vis_next[wi] = vw;
-      miss[wi] = 0;
-    }
+    if (wi < p.nwords && vw == ~0u) vis_next[wi] = vw;
+    uint32_t my_miss = 0;  // misses of word wbase + lane
     unsigned todo = __ballot_sync(FULL_MASK, vw != ~0u);
     while (todo) {
       int js[BU_WORDS];
@@ -265,12 +270,13 @@ __device__ void bu_pass_a(const RunParams& p, const uint32_t* __restrict__ vis_c
         const bool hit = active && pf[u] != NO_VERTEX && vis_test(vis_cur, pf[u]);
         const unsigned hits = __ballot_sync(FULL_MASK, hit);
         const unsigned misses = __ballot_sync(FULL_MASK, active && !hit);
-        if (js[u] >= 0 && lane == 0) {
-          vis_next[wbase + js[u]] = wv[u] | hits;
-          miss[wbase + js[u]] = misses;
-          found += __popc(hits);
-          scanned += __popc(~wv[u]);
-          nmiss += __popc(misses);
+        if (js[u] >= 0) {
+          if (lane == 0) vis_next[wbase + js[u]] = wv[u] | hits;
+          if (lane == js[u]) my_miss = misses;
+          if (lane == 0) {
+            found_a += __popc(hits);
+            scanned += __popc(~wv[u]);
+          }
         }
         if (hit) {
           const int64_t vr = (wbase + js[u]) * 32 + lane;
@@ -280,26 +286,9 @@ __device__ void bu_pass_a(const RunParams& p, const uint32_t* __restrict__ vis_c
         }
       }
     }
-  }
-  block_add(sh_acc, C_DISC, found);
-  block_add(sh_acc, C_SCAN, scanned);
-  block_add(sh_acc, C_QITEMS, nmiss);
-  if (p.count_edges) {  // a first-neighbour hit examined one edge (one sector)
-    block_add(sh_acc, C_EDGES, found);
-    block_add(sh_acc, C_SECT, found);
-  }
-}
-
-// Bottom-up pass B: the vertices whose first neighbour missed.  Each warp
-// gathers 32 of them into its lanes; a lane checks BU_SERIAL more row entries
-// alone, and rows still unresolved are scanned by the whole warp.
-__device__ void bu_pass_b(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* vis_next,
-                          const uint32_t* __restrict__ miss, unsigned long long* sh_acc, int64_t lvl) {
-  const int lane = threadIdx.x & 31;
-  unsigned long long found = 0, edges = 0, sectors = 0;
-  for (int64_t wbase = gwarp_id() * 32; wbase < p.nwords; wbase += gwarp_count() * 32) {
-    const int64_t wi = wbase + lane;
-    const uint32_t mw = wi < p.nwords ? __ldcg(miss + wi) : 0u;
+    // B: the vis_next words written above by lane 0 get the remaining finds by atomicOr
+    __syncwarp();
+    const uint32_t mw = my_miss;
     const uint32_t c = __popc(mw);
     const uint32_t incl = warp_incl_scan(c);
     const uint32_t excl = incl - c;
@@ -360,7 +349,7 @@ __device__ void bu_pass_b(const RunParams& p, const uint32_t* __restrict__ vis_c
         const int64_t val = (int64_t)__ldg(p.invert + parent) | lvl;
         if (p.deferred) p.pred_r[v] = val;
         else p.pred[__ldg(p.invert + v)] = val;
-        ++found;
+        ++found_b;
       }
       if (p.count_edges && v != NO_VERTEX) {
         edges += k;
@@ -368,10 +357,11 @@ __device__ void bu_pass_b(const RunParams& p, const uint32_t* __restrict__ vis_c
       }
     }
   }
-  block_add(sh_acc, C_DISC, found);
-  if (p.count_edges) {
-    block_add(sh_acc, C_EDGES, edges);
-    block_add(sh_acc, C_SECT, sectors);
+  block_add(sh_acc, C_DISC, found_a + found_b);
+  block_add(sh_acc, C_SCAN, scanned);
+  if (p.count_edges) {  // a first-neighbour hit examined one edge (one sector)
+    block_add(sh_acc, C_EDGES, found_a + edges);
+    block_add(sh_acc, C_SECT, found_a + sectors);
   }
 }
 
@@ -504,8 +494,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       listed = sh_cnt[C_QITEMS];
       mf = sh_cnt[C_MF];
     } else {
-      uint32_t* miss = reinterpret_cast<uint32_t*>(found_list);
-      bu_pass_a(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, sh_acc, lvl);
+      bu_level(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], sh_acc, lvl);
       if (!grid_sync<C_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
       if (tid == 0) t_mid = globaltimer();
       ++phase;
@@ -513,15 +502,6 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       scan = sh_cnt[C_SCAN];
       edges = sh_cnt[C_EDGES];
       sect = sh_cnt[C_SECT];
-      if (sh_cnt[C_QITEMS] > 0) {  // some first neighbours missed
-        unsigned long long* cnt_b = (NEXT_PHASE_SLOT());
-        bu_pass_b(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], miss, sh_acc, lvl);
-        if (!grid_sync<C_NUM>(&ctl->bar, cnt_b, sh_acc, cnt_b, sh_cnt, &sh_flag)) return;
-        ++phase;
-        disc += sh_cnt[C_DISC];
-        edges += sh_cnt[C_EDGES];
-        sect += sh_cnt[C_SECT];
-      }
     }
     const int64_t nq = (int64_t)disc;
     const int64_t carried_in = carried;
