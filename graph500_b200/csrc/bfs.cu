@@ -427,16 +427,19 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   // initialize_memory (bfs.hpp:241-276): pred = -1, visited = ~has_edge.  In
   // deferred mode pred is written whole by the final pass instead.
   if (tid == 0) ctl->t0_ns = globaltimer();
-  if (!p.deferred)
-    for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = -1;
-  for (int64_t i = tid; i < p.nwords; i += nthreads) p.vis[0][i] = p.vis_init[i];
-  if (blockIdx.x == 0 && threadIdx.x < 3 * C_NUM) (&ctl->cnt[0][0])[threadIdx.x] = 0;
+  // The root's own entries are written by the same fills, so one barrier
+  // separates initialisation from the first level.
   const uint32_t root_r = p.reorder[p.root];
   const bool has_edges = (int64_t)root_r < p.nlv && p.first[root_r] != NO_VERTEX;
   const uint64_t root_b = has_edges ? p.off[root_r] : 0;
   const uint64_t root_deg = has_edges ? p.off[root_r + 1] - root_b : 0;
   const int64_t root_items = (int64_t)chunks_of(root_deg);
-  if (!grid_sync<C_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
+  if (!p.deferred || !has_edges)  // deferred mode writes pred whole at the end
+    for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = i == p.root ? p.root : -1;
+  if (p.deferred && has_edges && tid == 0) p.pred_r[root_r] = p.root;
+  for (int64_t i = tid; i < p.nwords; i += nthreads)
+    p.vis[0][i] = p.vis_init[i] | (has_edges && i == (int64_t)(root_r >> 5) ? 1u << (root_r & 31) : 0u);
+  if (blockIdx.x == 0 && threadIdx.x < 3 * C_NUM) (&ctl->cnt[0][0])[threadIdx.x] = 0;
 
   // first_expand (bfs.hpp:477-518): the root's row becomes the first queue
   for (int64_t c = tid; c < root_items; c += nthreads) {
@@ -447,15 +450,8 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
     it.len = (uint32_t)(left < (uint64_t)TD_CHUNK ? left : (uint64_t)TD_CHUNK) | (c == 0 ? FIRST_CHUNK : 0u);
     items[c] = it;
   }
-  if (tid == 0) {
-    if (!p.deferred) p.pred[p.root] = p.root;
-    else if (has_edges) p.pred_r[root_r] = p.root;
-    if (has_edges) p.vis[0][root_r >> 5] |= 1u << (root_r & 31);
-    ctl->root_has_edges = has_edges ? 1 : 0;
-  }
-  if (!has_edges) {
-    if (p.deferred)  // the search is over before it starts: only the root has a parent
-      for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = i == p.root ? p.root : -1;
+  if (tid == 0) ctl->root_has_edges = has_edges ? 1 : 0;
+  if (!has_edges) {  // the search is over before it starts: only the root has a parent
     if (tid == 0) {
       ctl->num_levels = 0;
       ctl->final_vis = 0;

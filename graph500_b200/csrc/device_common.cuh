@@ -7,7 +7,7 @@
 
 namespace g500 {
 
-constexpr unsigned long long SPIN_LIMIT = 1ull << 25;  // ~ seconds of __nanosleep(64)
+constexpr unsigned long long SPIN_LIMIT = 1ull << 25;  // ~ seconds of polls with __nanosleep(32)
 
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
@@ -71,12 +71,32 @@ __device__ __forceinline__ void block_add(unsigned long long* sh_acc, int i, uns
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh_acc[i], v);
 }
 
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Grid-wide barrier for a cooperative launch.  The block's accumulated
-// counters are first added to flush_slot (one global atomic per counter per
-// block).  Thread 0 then arrives on a counter; the last arrival bumps the
-// generation.  Waiters spin with a bound; on timeout (or an error raised
-// elsewhere) the barrier reports failure and the caller returns.  On success
-// thread 0 copies read_slot into sh_cnt for the block's next decision.
+// counters are first added to flush_slot (one global atomic per non-zero
+// counter per block).  Thread 0 then arrives on a counter with acquire-release
+// semantics (the block's writes, ordered before it by __syncthreads, are
+// released with it); the last arrival resets the counter and publishes the
+// next generation with a release store; the others poll the generation and
+// take an acquire fence once it moved.  Polls are bounded; on timeout (or an error raised
+// elsewhere, checked every 16 polls) the barrier reports failure and the
+// caller returns.  On success thread 0 copies read_slot into sh_cnt for the
+// block's next decision.
 template <int NC>
 __device__ bool grid_sync(GridBarrier* bar, unsigned long long* flush_slot, unsigned long long* sh_acc,
                           const unsigned long long* read_slot, unsigned long long* sh_cnt, unsigned* sh_flag) {
@@ -88,28 +108,32 @@ __device__ bool grid_sync(GridBarrier* bar, unsigned long long* flush_slot, unsi
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = &bar->gen;
     volatile unsigned* err = &bar->err;
+    volatile unsigned* gen = &bar->gen;
     const unsigned g = *gen;
-    __threadfence();
     bool ok = true;
-    if (atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
-      bar->count = 0;
-      __threadfence();
-      atomicAdd(&bar->gen, 1u);
+    if (atom_add_acq_rel_gpu(&bar->count, 1u) == gridDim.x - 1) {
+      atomicExch(&bar->count, 0u);
+      st_release_gpu(&bar->gen, g + 1);
     } else {
+      // relaxed polls (an acquire per poll would invalidate L1 under the
+      // other blocks of the SM), one acquire fence once the generation moved
       unsigned long long spins = 0;
       while (*gen == g) {
-        if (*err) { ok = false; break; }
-        if (++spins > SPIN_LIMIT) {
+        ++spins;
+        if ((spins & 15) == 0 && *err) {
+          ok = false;
+          break;
+        }
+        if (spins > SPIN_LIMIT) {
           atomicOr(&bar->err, (unsigned)GRID_ERR_TIMEOUT);
           ok = false;
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
     }
-    __threadfence();
     if (*err) ok = false;
     *sh_flag = ok ? 1u : 0u;
     if (ok && read_slot) {
@@ -120,6 +144,5 @@ __device__ bool grid_sync(GridBarrier* bar, unsigned long long* flush_slot, unsi
   __syncthreads();
   return *sh_flag != 0;
 }
-
 
 }  // namespace g500
