@@ -51,7 +51,7 @@ constexpr uint64_t BFS_DEFERRED_PRED_BYTES = 64ull << 20;
 constexpr int BFS_MIN_BLOCKS = 2;        // co-resident blocks per SM (64 registers, no spills)
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
 constexpr int BU_WORDS = 8;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
-constexpr int BU_SERIAL = 6;              // row entries a lane checks alone before the warp helps
+constexpr int BU_SERIAL = 8;              // row entries a lane checks alone (one sector) before the warp helps
 
 struct RunParams {
   const uint64_t* __restrict__ off;
@@ -247,22 +247,28 @@ __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cu
                          unsigned long long* sh_acc, int64_t lvl) {
   const int lane = threadIdx.x & 31;
   unsigned long long found_a = 0, found_b = 0, scanned = 0, edges = 0, sectors = 0;
-  for (int64_t wbase = gwarp_id() * 32; wbase < p.nwords; wbase += gwarp_count() * 32) {
-    const int64_t wi = wbase + lane;
+  // lane l of warp w owns word w + (32 k + l) * nwarps: a warp's words are
+  // spread over the whole id range, so that the rows left for step B (under
+  // VERTEX_REORDERING=2 concentrated in some id ranges) spread over the warps
+  const int64_t nwarps = gwarp_count();
+  for (int64_t k32 = 0; gwarp_id() + k32 * nwarps < p.nwords; k32 += 32) {
+    const int64_t wi = gwarp_id() + (k32 + lane) * nwarps;
     const uint32_t vw = wi < p.nwords ? __ldg(vis_cur + wi) : ~0u;
     if (wi < p.nwords && vw == ~0u) vis_next[wi] = vw;
-    uint32_t my_miss = 0;  // misses of word wbase + lane
+    uint32_t my_miss = 0;  // misses of word wi
     unsigned todo = __ballot_sync(FULL_MASK, vw != ~0u);
     while (todo) {
       int js[BU_WORDS];
+      uint32_t wj[BU_WORDS];  // word index (nwords < 2^27)
       uint32_t wv[BU_WORDS], pf[BU_WORDS];
 #pragma unroll
       for (int u = 0; u < BU_WORDS; ++u) {
         js[u] = todo ? __ffs(todo) - 1 : -1;
         todo &= todo ? todo - 1 : 0u;
         wv[u] = __shfl_sync(FULL_MASK, vw, js[u] < 0 ? 0 : js[u]);
+        wj[u] = __shfl_sync(FULL_MASK, (uint32_t)wi, js[u] < 0 ? 0 : js[u]);
         if (js[u] < 0) wv[u] = ~0u;
-        pf[u] = ((wv[u] >> lane) & 1u) ? NO_VERTEX : __ldg(p.first + (wbase + js[u]) * 32 + lane);
+        pf[u] = ((wv[u] >> lane) & 1u) ? NO_VERTEX : __ldg(p.first + (int64_t)wj[u] * 32 + lane);
       }
 #pragma unroll
       for (int u = 0; u < BU_WORDS; ++u) {
@@ -271,7 +277,7 @@ __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cu
         const unsigned hits = __ballot_sync(FULL_MASK, hit);
         const unsigned misses = __ballot_sync(FULL_MASK, active && !hit);
         if (js[u] >= 0) {
-          if (lane == 0) vis_next[wbase + js[u]] = wv[u] | hits;
+          if (lane == 0) vis_next[wj[u]] = wv[u] | hits;
           if (lane == js[u]) my_miss = misses;
           if (lane == 0) {
             found_a += __popc(hits);
@@ -279,7 +285,7 @@ __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cu
           }
         }
         if (hit) {
-          const int64_t vr = (wbase + js[u]) * 32 + lane;
+          const int64_t vr = (int64_t)wj[u] * 32 + lane;
           const int64_t val = (int64_t)__ldg(p.invert + pf[u]) | lvl;
           if (p.deferred) p.pred_r[vr] = val;
           else p.pred[__ldg(p.invert + vr)] = val;
@@ -298,21 +304,30 @@ __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cu
       const int o = owner_lane(excl, idx);
       const uint32_t mwo = __shfl_sync(FULL_MASK, mw, o);
       const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
+      const uint32_t wo = __shfl_sync(FULL_MASK, (uint32_t)wi, o);
       uint32_t v = NO_VERTEX, parent = NO_VERTEX, k = 0;
       uint64_t pos = 0, end = 0;
       if (idx < total) {
-        v = (uint32_t)((wbase + o) * 32 + select_bit(mwo, idx - exo));
+        v = wo * 32 + select_bit(mwo, idx - exo);
         pos = __ldg(p.off + v) + 1;
         end = __ldg(p.off + v + 1);
         k = 1;
-        for (int s = 0; s < BU_SERIAL && pos < end; ++s, ++pos) {
-          const uint32_t cv = __ldg(p.col + pos);
-          ++k;
-          if (vis_test(vis_cur, cv)) {
-            parent = cv;
-            pos = end;
-            break;
-          }
+        // the next BU_SERIAL entries: loads first, then the visited tests
+        uint32_t cv[BU_SERIAL];
+#pragma unroll
+        for (int t = 0; t < BU_SERIAL; ++t) cv[t] = pos + t < end ? __ldg(p.col + pos + t) : NO_VERTEX;
+        int hit_t = -1;
+#pragma unroll
+        for (int t = BU_SERIAL - 1; t >= 0; --t)
+          if (cv[t] != NO_VERTEX && vis_test(vis_cur, cv[t])) hit_t = t;
+        if (hit_t >= 0) {
+          parent = cv[hit_t];
+          k += (uint32_t)hit_t + 1;
+          pos = end;
+        } else {
+          const uint64_t adv = end - pos < (uint64_t)BU_SERIAL ? end - pos : (uint64_t)BU_SERIAL;
+          k += (uint32_t)adv;
+          pos += adv;
         }
       }
       unsigned rest = __ballot_sync(FULL_MASK, pos < end);
