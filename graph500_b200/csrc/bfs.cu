@@ -47,7 +47,7 @@ constexpr int BFS_THREADS = 512;
 // coalesced, and one final pass writes pred in original-id order; writing
 // pred at random during the search costs a DRAM read-modify-write per
 // discovered vertex once pred no longer fits in L2.
-constexpr uint64_t BFS_DEFERRED_PRED_BYTES = 64ull << 20;
+constexpr uint64_t BFS_DEFERRED_PRED_BYTES = 100ull << 20;
 constexpr int BFS_MIN_BLOCKS = 2;        // co-resident blocks per SM (64 registers, no spills)
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
 constexpr int BU_WORDS = 8;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
