@@ -56,7 +56,7 @@ class LevelStats(C.Structure):
 class BfsStats(C.Structure):
     _fields_ = [("device_ms", C.c_double), ("host_ms", C.c_double), ("reached", C.c_int64), ("nedge", C.c_int64),
                 ("num_levels", C.c_int32), ("td_levels", C.c_int32), ("bu_levels", C.c_int32),
-                ("kernel_launches", C.c_int32)]
+                ("kernel_launches", C.c_int32), ("init_ms", C.c_double), ("search_ms", C.c_double)]
 
 
 class TuneResult(C.Structure):

@@ -63,6 +63,8 @@ struct RunParams {
   int64_t* __restrict__ pred;
   int64_t* __restrict__ pred_r;  // deferred mode: pred entries by reordered id, [nlv]
   int deferred;                  // write pred_r during the search, pred in one pass at the end
+  uint32_t first_id;             // mask of the vertex id in first[] (FIRST_ID, or all bits without flags)
+  uint32_t first_more;           // FIRST_MORE, or 0 when first[] has no flags (every miss is scanned)
   uint32_t* vis[2];
   TdItem* queue[2];
   BfsCtl* ctl;
@@ -246,7 +248,7 @@ __device__ __forceinline__ bool vis_test(const uint32_t* __restrict__ vis, uint3
 __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* __restrict__ vis_next,
                          unsigned long long* sh_acc, int64_t lvl) {
   const int lane = threadIdx.x & 31;
-  unsigned long long found_a = 0, found_b = 0, scanned = 0, edges = 0, sectors = 0;
+  unsigned long long found_a = 0, found_b = 0, scanned = 0, edges = 0, sectors = 0, single_misses = 0;
   // lane l of warp w owns word w + (32 k + l) * nwarps: a warp's words are
   // spread over the whole id range, so that the rows left for step B (under
   // VERTEX_REORDERING=2 concentrated in some id ranges) spread over the warps
@@ -273,9 +275,13 @@ __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cu
 #pragma unroll
       for (int u = 0; u < BU_WORDS; ++u) {
         const bool active = !((wv[u] >> lane) & 1u);  // every unvisited vertex has an edge
-        const bool hit = active && pf[u] != NO_VERTEX && vis_test(vis_cur, pf[u]);
+        const uint32_t fv = pf[u] & p.first_id;
+        const bool hit = active && pf[u] != NO_VERTEX && vis_test(vis_cur, fv);
+        // a row of one edge has nothing more to scan: its miss is final for this level
+        const bool more = p.first_more == 0 || (pf[u] & p.first_more);
         const unsigned hits = __ballot_sync(FULL_MASK, hit);
-        const unsigned misses = __ballot_sync(FULL_MASK, active && !hit);
+        const unsigned misses = __ballot_sync(FULL_MASK, active && !hit && more);
+        if (p.count_edges && active && !hit && !more) ++single_misses;
         if (js[u] >= 0) {
           if (lane == 0) vis_next[wj[u]] = wv[u] | hits;
           if (lane == js[u]) my_miss = misses;
@@ -286,7 +292,7 @@ __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cu
         }
         if (hit) {
           const int64_t vr = (int64_t)wj[u] * 32 + lane;
-          const int64_t val = (int64_t)__ldg(p.invert + pf[u]) | lvl;
+          const int64_t val = (int64_t)__ldg(p.invert + fv) | lvl;
           if (p.deferred) p.pred_r[vr] = val;
           else p.pred[__ldg(p.invert + vr)] = val;
         }
@@ -374,9 +380,9 @@ __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cu
   }
   block_add(sh_acc, C_DISC, found_a + found_b);
   block_add(sh_acc, C_SCAN, scanned);
-  if (p.count_edges) {  // a first-neighbour hit examined one edge (one sector)
-    block_add(sh_acc, C_EDGES, found_a + edges);
-    block_add(sh_acc, C_SECT, found_a + sectors);
+  if (p.count_edges) {  // a first-neighbour hit or a one-edge miss examined one edge (one sector)
+    block_add(sh_acc, C_EDGES, found_a + single_misses + edges);
+    block_add(sh_acc, C_SECT, found_a + single_misses + sectors);
   }
 }
 
@@ -772,6 +778,8 @@ extern "C" int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_o
   p.off = g->d_offsets;
   p.col = g->d_cols;
   p.first = g->d_first;
+  p.first_id = g->first_flags ? FIRST_ID : 0xFFFFFFFFu;
+  p.first_more = g->first_flags ? FIRST_MORE : 0u;
   p.invert = g->d_invert;
   p.reorder = g->d_reorder;
   p.vis_init = g->d_vis_init;
@@ -833,6 +841,8 @@ extern "C" int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_o
     }
     stats->num_levels = (int32_t)c.num_levels;
     stats->kernel_launches = 1;
+    if (c.t_init_ns >= c.t0_ns) stats->init_ms = (double)(c.t_init_ns - c.t0_ns) * 1e-6;
+    if (c.t_end_ns >= c.t_init_ns) stats->search_ms = (double)(c.t_end_ns - c.t_init_ns) * 1e-6;
     if (c.num_levels) {
       std::vector<LevelRecord> rec(c.num_levels);
       G500_CUDA(cudaMemcpy(rec.data(), b->d_rec, sizeof(LevelRecord) * c.num_levels, cudaMemcpyDeviceToHost));

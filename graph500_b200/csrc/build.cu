@@ -188,11 +188,11 @@ __global__ void __launch_bounds__(CP_THREADS) unique_write_kernel(const uint64_t
 }
 
 __global__ void finish_rows_kernel(const uint64_t* __restrict__ offsets, const uint32_t* __restrict__ cols,
-                                   int64_t nlv, uint32_t* first, uint32_t* vis_init) {
+                                   int64_t nlv, int flags, uint32_t* first, uint32_t* vis_init) {
   const int lane = threadIdx.x & 31;
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nlv; v += (int64_t)gridDim.x * blockDim.x) {
     uint64_t b = offsets[v], e = offsets[v + 1];
-    first[v] = e > b ? cols[b] : NO_VERTEX;
+    first[v] = e > b ? (cols[b] | (flags && e - b > 1 ? FIRST_MORE : 0u)) : NO_VERTEX;
     unsigned none = __ballot_sync(FULL_MASK, e == b);  // nlv is a multiple of 32
     if (lane == 0) vis_init[v >> 5] = none;
   }
@@ -348,7 +348,9 @@ static int build_from_device_edges(g500_graph* g, const g500_packed_edge* d_edge
     G500_CUDA(cudaGetLastError());
   }
   if (nlv > 0) {
-    finish_rows_kernel<<<grid_for(nlv), 256, 0, s>>>(g->d_offsets, g->d_cols, nlv, g->d_first, g->d_vis_init);
+    g->first_flags = nlv <= (int64_t)FIRST_ID;
+    finish_rows_kernel<<<grid_for(nlv), 256, 0, s>>>(g->d_offsets, g->d_cols, nlv, g->first_flags ? 1 : 0,
+                                                     g->d_first, g->d_vis_init);
     G500_CUDA(cudaGetLastError());
   }
   G500_CUDA(cudaStreamSynchronize(s));

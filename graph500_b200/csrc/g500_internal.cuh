@@ -32,6 +32,11 @@ constexpr unsigned FULL_MASK = 0xFFFFFFFFu;
 constexpr int64_t LOCAL_VERTS_UNIT = 65536;  // max(11, 16) bits, bfs.hpp:109 + graph_constructor.hpp:557
 constexpr int TD_CHUNK = 128;                // edges per top-down work item (one warp pass)
 constexpr uint32_t NO_VERTEX = 0xFFFFFFFFu;
+// first[v] of a row with more than one edge carries FIRST_MORE (when the graph
+// has first_flags: every reordered id then fits in 31 bits), so that a
+// bottom-up miss on a one-edge row needs no further scan
+constexpr uint32_t FIRST_MORE = 0x80000000u;
+constexpr uint32_t FIRST_ID = 0x7FFFFFFFu;
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 inline int64_t roundup(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
@@ -99,7 +104,8 @@ struct g500_graph {
 
   uint64_t* d_offsets = nullptr;    // [nlv + 1]
   uint32_t* d_cols = nullptr;       // [nge]   reordered targets, ascending per row
-  uint32_t* d_first = nullptr;      // [nlv]   first (smallest) neighbour or NO_VERTEX
+  uint32_t* d_first = nullptr;      // [nlv]   first (smallest) neighbour (| FIRST_MORE) or NO_VERTEX
+  bool first_flags = false;         // first[] carries FIRST_MORE (nlv <= FIRST_ID)
   uint32_t* d_reorder = nullptr;    // [nolv]  original -> reordered
   uint32_t* d_invert = nullptr;     // [nolv]  reordered -> original
   uint32_t* d_vis_init = nullptr;   // [nlv/32] ~has_edge in reordered space

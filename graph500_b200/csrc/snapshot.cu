@@ -18,7 +18,7 @@ namespace g500 {
 namespace {
 
 constexpr char SNAP_MAGIC[8] = {'G', '5', '0', '0', 'C', 'S', 'R', '1'};
-constexpr uint32_t SNAP_VERSION = 1;
+constexpr uint32_t SNAP_VERSION = 2;  // 2: first[] carries FIRST_MORE
 constexpr size_t SNAP_CHUNK = 64u << 20;  // staging buffer for the copies
 
 enum SnapArray { S_OFFSETS, S_COLS, S_FIRST, S_REORDER, S_INVERT, S_VIS_INIT, S_ENDP, S_HAS_EDGE, S_EDGES, S_NUM };
@@ -28,7 +28,7 @@ struct SnapHeader {
   uint32_t version;
   int32_t reorder_mode;
   int32_t log_bits;
-  int32_t pad;
+  int32_t first_flags;
   int64_t log_orig_global_verts, nolv, nlv, ngv, nge, max_used_vertex, num_edges, device_bytes;
   double gen_seconds, build_seconds;
   uint64_t bytes[S_NUM];
@@ -98,6 +98,7 @@ extern "C" int g500_graph_save(const g500_graph* g, const char* path) {
   h.version = SNAP_VERSION;
   h.reorder_mode = g->reorder_mode;
   h.log_bits = g->log_bits;
+  h.first_flags = g->first_flags ? 1 : 0;
   h.log_orig_global_verts = g->log_orig_global_verts;
   h.nolv = g->nolv;
   h.nlv = g->nlv;
@@ -148,6 +149,7 @@ extern "C" int g500_graph_load(const char* path, int device, g500_graph** out) {
   g500_graph* g = nullptr;
   G500_TRY(new_graph(device, h.reorder_mode, &g));
   g->log_bits = h.log_bits;
+  g->first_flags = h.first_flags != 0;
   g->log_orig_global_verts = h.log_orig_global_verts;
   g->nolv = h.nolv;
   g->nlv = h.nlv;

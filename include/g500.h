@@ -147,6 +147,8 @@ typedef struct g500_bfs_stats {
   int32_t td_levels;
   int32_t bu_levels;
   int32_t kernel_launches; /* kernels this library launched for the run */
+  double init_ms;          /* device global timer: kernel start to the first level */
+  double search_ms;        /* device global timer: the levels (and the deferred pred pass) */
 } g500_bfs_stats;
 
 /* BfsBase::prepare_bfs / allocate_memory (bfs.hpp:115-118, :151-239). */

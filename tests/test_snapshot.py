@@ -21,7 +21,7 @@ def test_foreign_file_is_refused(g500, tmp_path):
 
 def test_inconsistent_header_is_refused(g500, tmp_path):
     # right magic and version, lengths that do not match the scalars
-    hdr = b"G500CSR1" + struct.pack("<Iiii", 1, 2, 20, 0) + struct.pack("<8q", 16, 65536, 65536, 10, 100, 9, 0, 0)
+    hdr = b"G500CSR1" + struct.pack("<Iiii", 2, 2, 20, 1) + struct.pack("<8q", 16, 65536, 65536, 10, 100, 9, 0, 0)
     hdr += struct.pack("<2d", 0.0, 0.0) + struct.pack("<9Q", *([1] * 9))
     p = tmp_path / "bad.g500"
     p.write_bytes(hdr)
