@@ -86,7 +86,8 @@ class MsLevel(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("max_batch", C.c_int32), ("max_workers_per_graph", C.c_int32), ("mode", C.c_int32),
-                ("vertices_per_block", C.c_int32), ("hbm_reserve_bytes", C.c_uint64), ("alpha", C.c_double)]
+                ("vertices_per_block", C.c_int32), ("hbm_reserve_bytes", C.c_uint64), ("alpha", C.c_double),
+                ("max_grid_fraction", C.c_double)]
 
 
 class QueryResult(C.Structure):

@@ -363,6 +363,7 @@ extern "C" int g500_server_default_config(g500_server_config* cfg) {
   cfg->vertices_per_block = 4096;
   cfg->hbm_reserve_bytes = 1ull << 30;
   cfg->alpha = 6.0;
+  cfg->max_grid_fraction = 0.5;
   return G500_OK;
 }
 
@@ -377,6 +378,7 @@ extern "C" int g500_server_create(g500_graph* const* graphs, int num_graphs, con
   if (c.mode != G500_SERVE_BATCHED && c.mode != G500_SERVE_PLAIN) return g500::set_error(G500_E_INVAL, "unknown mode");
   if (c.vertices_per_block < 1) c.vertices_per_block = 4096;
   if (!(c.alpha > 0)) c.alpha = 6.0;
+  if (!(c.max_grid_fraction > 0) || c.max_grid_fraction > 1) c.max_grid_fraction = 1.0;
   for (int i = 0; i < num_graphs; ++i) {
     if (!graphs[i]) return g500::set_error(G500_E_INVAL, "graph %d is null", i);
     if (graphs[i]->device != graphs[0]->device) return g500::set_error(G500_E_INVAL, "graphs on different devices");
@@ -406,7 +408,8 @@ extern "C" int g500_server_create(g500_graph* const* graphs, int num_graphs, con
       if (st == G500_OK) {
         s->capacity = s->capacity == 0 ? full : std::min(s->capacity, full);
         const int64_t want = (graphs[g]->nlv + c.vertices_per_block - 1) / c.vertices_per_block;
-        s->blocks[(size_t)g] = (int)std::max<int64_t>(std::min<int64_t>(want, full), std::min(16, full));
+        const int64_t cap = std::max<int64_t>(1, (int64_t)(c.max_grid_fraction * full));
+        s->blocks[(size_t)g] = (int)std::max<int64_t>(std::min<int64_t>(want, cap), std::min<int64_t>(16, cap));
         st = g500_msbfs_set_params(w.ms, 64, c.alpha, 1);
       }
       if (st == G500_OK) st = g500_msbfs_set_root_stats(w.ms, 1);

@@ -311,6 +311,8 @@ typedef struct g500_server_config {
   int32_t vertices_per_block;    /* grid of a graph's launches: ceil(num_local_verts / this), >= 16 blocks */
   uint64_t hbm_reserve_bytes;    /* free device memory a new launch slot must leave */
   double alpha;                  /* multi-source direction threshold (g500_msbfs_set_params) */
+  double max_grid_fraction;      /* a launch uses at most this share of the device's co-resident blocks
+                                    (so that launches of other graphs run beside it); (0, 1] */
 } g500_server_config;
 
 typedef struct g500_query_result {
