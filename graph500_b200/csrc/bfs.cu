@@ -570,16 +570,37 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
 #undef NEXT_PHASE_SLOT
   if (p.deferred) {
     // pred in original-id order, sequential writes: a reached vertex (visited
-    // now, not pre-visited for lack of edges) takes its entry from pred_r
+    // now, not pre-visited for lack of edges) takes its entry from pred_r.
+    // 8 consecutive vertices per thread, all loads of a step issued together;
+    // the streamed map and pred bypass L2 retention (evict-first), so that the
+    // gathered bitmaps and pred_r stay cached.  nolv is a multiple of 65536.
     const uint32_t* vf = p.vis[cur_vis];
-    for (int64_t u = tid; u < p.nolv; u += nthreads) {
-      const uint32_t r = __ldg(p.reorder + u);
-      int64_t val = -1;
-      if ((int64_t)r < p.nlv) {
-        const uint32_t bit = 1u << (r & 31);
-        if ((__ldcg(vf + (r >> 5)) & ~__ldg(p.vis_init + (r >> 5))) & bit) val = __ldcg(p.pred_r + r);
+    if (reinterpret_cast<uintptr_t>(p.pred) & 15) {  // a caller's pred not 16-byte aligned: one entry at a time
+      for (int64_t u = tid; u < p.nolv; u += nthreads) {
+        const uint32_t r = __ldg(p.reorder + u);
+        int64_t val = -1;
+        if ((int64_t)r < p.nlv && (((__ldcg(vf + (r >> 5)) & ~__ldg(p.vis_init + (r >> 5))) >> (r & 31)) & 1u))
+          val = __ldcg(p.pred_r + r);
+        p.pred[u] = val;
       }
-      p.pred[u] = val;
+    } else
+    for (int64_t u0 = tid * 8; u0 < p.nolv; u0 += nthreads * 8) {
+      const uint4 ra = __ldcs(reinterpret_cast<const uint4*>(p.reorder + u0));
+      const uint4 rb = __ldcs(reinterpret_cast<const uint4*>(p.reorder + u0 + 4));
+      const uint32_t r[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
+      bool reach[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        reach[i] = false;
+        if ((int64_t)r[i] < p.nlv)
+          reach[i] = ((__ldcg(vf + (r[i] >> 5)) & ~__ldg(p.vis_init + (r[i] >> 5))) >> (r[i] & 31)) & 1u;
+      }
+      long long val[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) val[i] = reach[i] ? (long long)__ldcg(p.pred_r + r[i]) : -1ll;
+      longlong2* dst = reinterpret_cast<longlong2*>(p.pred + u0);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) __stcs(dst + i, make_longlong2(val[2 * i], val[2 * i + 1]));
     }
   }
   if (tid == 0) {
