@@ -181,6 +181,7 @@ def lib() -> C.CDLL:
         "g500_msbfs_set_grid": ([P, i32], i32),
         "g500_msbfs_get_grid": ([P, i32, C.POINTER(i32), C.POINTER(i32)], i32),
         "g500_msbfs_workspace_bytes": ([P, C.POINTER(u64)], i32),
+        "g500_selftest_barrier_timeout": ([i32, C.POINTER(i32), C.POINTER(i32)], i32),
         "g500_server_default_config": ([C.POINTER(ServerConfig)], i32),
         "g500_server_create": ([P, i32, C.POINTER(ServerConfig), C.POINTER(P)], i32),
         "g500_server_submit": ([P, i32, i64, u64, P, C.POINTER(i64)], i32),

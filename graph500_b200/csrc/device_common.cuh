@@ -99,7 +99,8 @@ __device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
 // block's next decision.
 template <int NC>
 __device__ bool grid_sync(GridBarrier* bar, unsigned long long* flush_slot, unsigned long long* sh_acc,
-                          const unsigned long long* read_slot, unsigned long long* sh_cnt, unsigned* sh_flag) {
+                          const unsigned long long* read_slot, unsigned long long* sh_cnt, unsigned* sh_flag,
+                          unsigned long long spin_limit = SPIN_LIMIT) {
   __syncthreads();
   if (threadIdx.x < NC) {
     const unsigned long long v = sh_acc[threadIdx.x];
@@ -125,7 +126,7 @@ __device__ bool grid_sync(GridBarrier* bar, unsigned long long* flush_slot, unsi
           ok = false;
           break;
         }
-        if (spins > SPIN_LIMIT) {
+        if (spins > spin_limit) {
           atomicOr(&bar->err, (unsigned)GRID_ERR_TIMEOUT);
           ok = false;
           break;

@@ -369,6 +369,12 @@ int g500_server_run_poisson(g500_server* s, double rate_qps, int64_t num_queries
                             g500_serve_report* rep);
 int g500_server_destroy(g500_server* s);
 
+/* Self-test of the failure path of the bounded grid barrier (no counterpart in
+ * the reference): a cooperative launch in which one block never arrives must
+ * end with the others giving up (*timed_out = 1) and leave the context usable
+ * for a following launch (*recovered = 1).  Causes no fault. */
+int g500_selftest_barrier_timeout(int device, int* timed_out, int* recovered);
+
 /* Validation that allocates nothing, for callers that cannot call cudaMalloc
  * (a host framework owning all device memory through its own arena or caching
  * allocator, or a serving loop that forbids allocation after start-up).  No
