@@ -87,7 +87,7 @@ class MsLevel(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("max_batch", C.c_int32), ("max_workers_per_graph", C.c_int32), ("mode", C.c_int32),
                 ("vertices_per_block", C.c_int32), ("hbm_reserve_bytes", C.c_uint64), ("alpha", C.c_double),
-                ("max_grid_fraction", C.c_double)]
+                ("max_grid_fraction", C.c_double), ("plain_below", C.c_int32), ("pad", C.c_int32)]
 
 
 class QueryResult(C.Structure):
@@ -160,6 +160,7 @@ def lib() -> C.CDLL:
         "g500_bfs_set_params": ([P, C.c_double, C.c_double, i32], i32),
         "g500_bfs_set_stream": ([P, P], i32),
         "g500_bfs_set_pred_mode": ([P, i32], i32),
+        "g500_bfs_set_grid": ([P, i32], i32),
         "g500_bfs_set_policy": ([P, i32], i32),
         "g500_bfs_autotune": ([P, P, i32, i32, C.POINTER(TuneResult)], i32),
         "g500_bfs_run": ([P, i64, P, i32, C.POINTER(BfsStats)], i32),

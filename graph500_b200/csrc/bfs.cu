@@ -643,6 +643,9 @@ static int bfs_free(g500_bfs* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   dev_free(b->d_pred);
   dev_free(b->d_pred_r);
+  dev_free(b->d_levels);
+  dev_free(b->d_overflow);
+  if (b->ev_done) cudaEventDestroy(b->ev_done);
   dev_free(b->d_vis[0]);
   dev_free(b->d_vis[1]);
   dev_free(b->d_queue[0]);
@@ -655,6 +658,56 @@ static int bfs_free(g500_bfs* b) {
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
   delete b;
   return G500_OK;
+}
+
+// The kernel's parameters for one run from `root` writing pred to `pred`.
+static int make_params(g500_bfs* b, int64_t root, int64_t* pred, RunParams* out) {
+  g500_graph* g = b->g;
+  RunParams& p = *out;
+  p.off = g->d_offsets;
+  p.col = g->d_cols;
+  p.first = g->d_first;
+  p.first_id = g->first_flags ? FIRST_ID : 0xFFFFFFFFu;
+  p.first_more = g->first_flags ? FIRST_MORE : 0u;
+  p.invert = g->d_invert;
+  p.reorder = g->d_reorder;
+  p.vis_init = g->d_vis_init;
+  p.pred = pred;
+  p.deferred = b->pred_mode == 2 || (b->pred_mode == 0 && (uint64_t)g->nolv * 8 > BFS_DEFERRED_PRED_BYTES);
+  if (p.deferred && !b->d_pred_r) G500_TRY(dev_alloc_n(&b->d_pred_r, std::max<int64_t>(g->nlv, 1), "deferred pred"));
+  p.pred_r = b->d_pred_r;
+  p.vis[0] = b->d_vis[0];
+  p.vis[1] = b->d_vis[1];
+  p.queue[0] = b->d_queue[0];
+  p.queue[1] = b->d_queue[1];
+  p.ctl = b->d_ctl;
+  p.rec = b->d_rec;
+  p.nolv = g->nolv;
+  p.nlv = g->nlv;
+  p.nwords = g->nlv / 32;
+  p.ngv = g->ngv;
+  p.cap = b->queue_cap;
+  p.root = root;
+  p.alpha = b->alpha;
+  p.policy = b->policy;
+  p.beta = b->beta;
+  p.count_edges = b->count_edges;
+  return G500_OK;
+}
+
+// pred -> uint8 levels (255 unreached); a level over 254 raises *overflow
+__global__ void levels_from_pred_kernel(const int64_t* __restrict__ pred, int64_t n, uint8_t* __restrict__ out,
+                                        unsigned* overflow) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = pred[i];
+    uint8_t l = 255;
+    if (v != -1) {
+      const int64_t lv = (v >> 48) & 0xFFFF;
+      if (lv > 254) atomicOr(overflow, 1u);
+      l = (uint8_t)(lv > 254 ? 254 : lv);
+    }
+    out[i] = l;
+  }
 }
 
 extern "C" int g500_bfs_create(g500_graph* g, g500_bfs** out) {
@@ -690,7 +743,7 @@ extern "C" int g500_bfs_create(g500_graph* g, g500_bfs** out) {
     chk(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, g->device), "cudaDeviceGetAttribute");
     if (st == G500_OK && (!coop || per_sm <= 0))
       st = set_error(G500_E_DEVICE, "device cannot co-schedule the persistent BFS kernel");
-    b->grid = (unsigned)(num_sms() * std::max(per_sm, 1));
+    b->grid = b->grid_full = (unsigned)(num_sms() * std::max(per_sm, 1));
   }
   if (st != G500_OK) {
     bfs_free(b);
@@ -699,6 +752,90 @@ extern "C" int g500_bfs_create(g500_graph* g, g500_bfs** out) {
   *out = b;
   return G500_OK;
 }
+
+extern "C" int g500_bfs_set_grid(g500_bfs* b, int blocks) {
+  if (!b) return set_error(G500_E_INVAL, "null bfs");
+  if (blocks < 0) return set_error(G500_E_INVAL, "negative block count");
+  if (b->in_flight) return set_error(G500_E_STATE, "a run is in flight");
+  b->grid = blocks == 0 ? b->grid_full : std::min<unsigned>((unsigned)blocks, b->grid_full);
+  return G500_OK;
+}
+
+namespace g500 {
+
+int bfs_launch_levels(g500_bfs* b, int64_t root, uint8_t* levels_dst) {
+  if (!b) return set_error(G500_E_INVAL, "null bfs");
+  if (b->in_flight) return set_error(G500_E_STATE, "the previous run has not completed");
+  g500_graph* g = b->g;
+  if (root < 0 || root >= g->nolv)
+    return set_error(G500_E_INVAL, "root %lld outside [0, %lld)", (long long)root, (long long)g->nolv);
+  G500_CUDA(cudaSetDevice(g->device));
+  if (!b->d_levels) G500_TRY(dev_alloc_n(&b->d_levels, std::max<int64_t>(g->nolv, 1), "levels"));
+  if (!b->d_overflow) G500_TRY(dev_alloc_n(&b->d_overflow, 1, "level overflow flag"));
+  if (!b->ev_done) G500_CUDA(cudaEventCreateWithFlags(&b->ev_done, cudaEventDisableTiming));
+  cudaStream_t s = b->stream;
+  RunParams p;
+  G500_TRY(make_params(b, root, b->d_pred, &p));
+  void* args[] = {&p};
+  G500_CUDA(cudaMemsetAsync(b->d_ctl, 0, sizeof(BfsCtl), s));
+  G500_CUDA(cudaMemsetAsync(b->d_overflow, 0, sizeof(unsigned), s));
+  G500_CUDA(cudaLaunchCooperativeKernel((const void*)bfs_persistent_kernel, dim3(b->grid), dim3(BFS_THREADS), args,
+                                        0, s));
+  const unsigned rg = (unsigned)std::min<int64_t>(ceil_div(std::max<int64_t>(p.nwords, 1), 256), num_sms() * 8);
+  reach_kernel<<<rg, 256, 0, s>>>(b->d_vis[0], b->d_vis[1], g->d_vis_init, g->d_endp, p.nwords, b->d_ctl);
+  const unsigned lg = (unsigned)std::min<int64_t>(ceil_div(g->nolv, 256), num_sms() * 8);
+  levels_from_pred_kernel<<<lg, 256, 0, s>>>(b->d_pred, g->nolv, b->d_levels, b->d_overflow);
+  G500_CUDA(cudaGetLastError());
+  if (levels_dst) G500_CUDA(cudaMemcpyAsync(levels_dst, b->d_levels, (size_t)g->nolv, cudaMemcpyDefault, s));
+  G500_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s));
+  G500_CUDA(cudaMemcpyAsync(&b->h_ctl->pad_overflow, b->d_overflow, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  G500_CUDA(cudaEventRecord(b->ev_done, s));
+  b->last_root = root;
+  b->in_flight = 1;
+  return G500_OK;
+}
+
+int bfs_poll(g500_bfs* b, int* done) {
+  if (!b || !done) return set_error(G500_E_INVAL, "null argument");
+  if (!b->in_flight) return set_error(G500_E_STATE, "no run in flight");
+  const cudaError_t e = cudaEventQuery(b->ev_done);
+  if (e == cudaSuccess) {
+    *done = 1;
+    return G500_OK;
+  }
+  if (e == cudaErrorNotReady) {
+    *done = 0;
+    return G500_OK;
+  }
+  return cuda_error(e, "cudaEventQuery", __FILE__, __LINE__);
+}
+
+int bfs_complete(g500_bfs* b, int64_t* reached, int64_t* nedge) {
+  if (!b) return set_error(G500_E_INVAL, "null bfs");
+  if (!b->in_flight) return set_error(G500_E_STATE, "no run in flight");
+  b->in_flight = 0;
+  G500_CUDA(cudaSetDevice(b->g->device));
+  const cudaError_t e = cudaEventSynchronize(b->ev_done);
+  if (e != cudaSuccess) return cuda_error(e, "cudaEventSynchronize", __FILE__, __LINE__);
+  const BfsCtl& c = *b->h_ctl;
+  if (c.bar.err & BFS_ERR_TIMEOUT) return set_error(G500_E_TIMEOUT, "grid barrier wait gave up (bounded spin)");
+  if (c.bar.err & BFS_ERR_QUEUE) return set_error(G500_E_RANGE, "top-down queue overflow");
+  if (c.bar.err & BFS_ERR_DEPTH) return set_error(G500_E_RANGE, "BFS depth exceeds the 16-bit level field");
+  if (c.pad_overflow) return set_error(G500_E_RANGE, "a level over 254 does not fit the uint8 levels");
+  if (c.root_has_edges) {
+    if (reached) *reached = (int64_t)c.reach[0];
+    if (nedge) *nedge = (int64_t)(c.reach[1] / 2);
+  } else {  // a root without edges reached only itself; its self-loops are its edges
+    uint32_t root_r = 0, ep = 0;
+    G500_CUDA(cudaMemcpy(&root_r, b->g->d_reorder + b->last_root, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    G500_CUDA(cudaMemcpy(&ep, b->g->d_endp + root_r, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (reached) *reached = 1;
+    if (nedge) *nedge = ep / 2;
+  }
+  return G500_OK;
+}
+
+}  // namespace g500
 
 extern "C" int g500_bfs_set_params(g500_bfs* b, double alpha, double beta, int count_edges) {
   if (!b) return set_error(G500_E_INVAL, "null bfs");
@@ -796,34 +933,7 @@ extern "C" int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_o
   auto t0 = std::chrono::steady_clock::now();
   cudaStream_t s = b->stream;
   RunParams p;
-  p.off = g->d_offsets;
-  p.col = g->d_cols;
-  p.first = g->d_first;
-  p.first_id = g->first_flags ? FIRST_ID : 0xFFFFFFFFu;
-  p.first_more = g->first_flags ? FIRST_MORE : 0u;
-  p.invert = g->d_invert;
-  p.reorder = g->d_reorder;
-  p.vis_init = g->d_vis_init;
-  p.pred = pred_on_device ? pred : b->d_pred;
-  p.deferred = b->pred_mode == 2 || (b->pred_mode == 0 && (uint64_t)g->nolv * 8 > BFS_DEFERRED_PRED_BYTES);
-  if (p.deferred && !b->d_pred_r) G500_TRY(dev_alloc_n(&b->d_pred_r, std::max<int64_t>(g->nlv, 1), "deferred pred"));
-  p.pred_r = b->d_pred_r;
-  p.vis[0] = b->d_vis[0];
-  p.vis[1] = b->d_vis[1];
-  p.queue[0] = b->d_queue[0];
-  p.queue[1] = b->d_queue[1];
-  p.ctl = b->d_ctl;
-  p.rec = b->d_rec;
-  p.nolv = g->nolv;
-  p.nlv = g->nlv;
-  p.nwords = g->nlv / 32;
-  p.ngv = g->ngv;
-  p.cap = b->queue_cap;
-  p.root = root;
-  p.alpha = b->alpha;
-  p.policy = b->policy;
-  p.beta = b->beta;
-  p.count_edges = b->count_edges;
+  G500_TRY(make_params(b, root, pred_on_device ? pred : b->d_pred, &p));
   void* args[] = {&p};
   G500_CUDA(cudaMemsetAsync(b->d_ctl, 0, sizeof(BfsCtl), s));
   G500_CUDA(cudaEventRecord(b->ev0, s));

@@ -149,6 +149,7 @@ struct BfsCtl {
   unsigned long long t_init_ns;  // pred/visited initialised and root seeded
   unsigned long long t_end_ns;
   unsigned long long reach[2];  // reached vertices, 2 * nedge (filled by reach_kernel)
+  unsigned pad_overflow;        // host copy of the levels-overflow flag of an asynchronous run
 };
 
 // One record per level, written by the kernel.
@@ -173,6 +174,11 @@ struct g500_bfs {
 
   int64_t* d_pred = nullptr;         // [nolv]
   int64_t* d_pred_r = nullptr;       // [nlv] deferred mode: pred entries by reordered id
+  uint8_t* d_levels = nullptr;       // [nolv] levels of an asynchronous run (serving)
+  unsigned* d_overflow = nullptr;    // a level over 254 in d_levels
+  cudaEvent_t ev_done = nullptr;
+  int in_flight = 0;
+  unsigned grid_full = 0;            // every co-resident block of the device
   int pred_mode = 0;                 // 0 by pred size, 1 direct, 2 deferred
   uint32_t* d_vis[2] = {nullptr, nullptr};
   TdItem* d_queue[2] = {nullptr, nullptr};
@@ -185,6 +191,13 @@ struct g500_bfs {
 };
 
 namespace g500 {
+// Asynchronous plain BFS for the serving loop: the run from `root`, its uint8
+// levels (255 unreached) into levels_dst (host or device, may be null), the
+// reached / edge counts, all enqueued on the handle's stream.
+int bfs_launch_levels(g500_bfs* b, int64_t root, uint8_t* levels_dst);
+int bfs_poll(g500_bfs* b, int* done);
+int bfs_complete(g500_bfs* b, int64_t* reached, int64_t* nedge);
+
 // g500_msbfs_launch that also copies each root's level row (pred_size bytes)
 // to root_dsts[i] when it is not null, before the launch's completion event.
 int msbfs_launch_to(g500_msbfs* m, const int64_t* roots, int nroots, uint8_t* const* root_dsts);

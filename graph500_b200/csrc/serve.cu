@@ -53,6 +53,16 @@ struct Worker {
   std::vector<int64_t> qids;
 };
 
+// A plain BFS handle that serves one query at a time, for graphs whose queue
+// is short: a one-root multi-source launch costs far more than one BFS.
+struct PlainWorker {
+  g500_bfs* bfs = nullptr;
+  bool busy = false;
+  int units = 0;  // share of the block budget (in 256-thread blocks)
+  double t_start_us = 0;
+  int64_t qid = -1;
+};
+
 uint64_t splitmix64(uint64_t* x) {
   uint64_t z = (*x += 0x9E3779B97F4A7C15ull);
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -84,6 +94,10 @@ struct g500_server {
 
   // engine thread only
   std::vector<std::vector<Worker>> workers;
+  std::vector<std::vector<PlainWorker>> pworkers;  // per graph
+  std::vector<int> plain_below;    // queues up to this long go to plain BFS runs
+  std::vector<int> pblocks;        // grid of a graph's plain runs (512-thread blocks)
+  std::vector<uint64_t> pws_bytes; // workspace of one plain handle
   std::vector<int> blocks;         // grid of each graph's launches
   std::vector<double> alpha;
   std::vector<uint64_t> ws_bytes;  // workspace of one worker
@@ -159,6 +173,23 @@ int new_worker(g500_server* s, int g, Worker* out) {
 // Poll the busy workers; returns whether any finished.
 bool reap(g500_server* s) {
   bool any = false;
+  for (auto& ps : s->pworkers)
+    for (PlainWorker& w : ps) {
+      if (!w.busy) continue;
+      int done = 0;
+      int st = g500::bfs_poll(w.bfs, &done);
+      if (st == G500_OK && !done) continue;
+      int64_t reached = 0, nedge = 0;
+      const int st2 = g500::bfs_complete(w.bfs, &reached, &nedge);
+      if (st == G500_OK) st = st2;
+      const std::vector<int64_t> ids{w.qid};
+      finish_queries(s, ids, st, &reached, &nedge, w.t_start_us, 1, 0);
+      w.busy = false;
+      w.qid = -1;
+      s->inflight_blocks -= w.units;
+      s->in_flight.fetch_sub(1);
+      any = true;
+    }
   for (auto& ws : s->workers)
     for (Worker& w : ws) {
       if (!w.busy) continue;
@@ -190,6 +221,52 @@ bool dispatch(g500_server* s) {
       {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->pending[(size_t)g].empty()) break;
+      }
+      size_t waiting;
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        waiting = s->pending[(size_t)g].size();
+      }
+      if ((int)waiting <= s->plain_below[(size_t)g] && !s->pworkers[(size_t)g].empty()) {
+        // a short queue: one plain BFS per query
+        PlainWorker* pw = nullptr;
+        for (PlainWorker& x : s->pworkers[(size_t)g])
+          if (!x.busy) {
+            pw = &x;
+            break;
+          }
+        if (pw && s->inflight_blocks + pw->units <= s->capacity) {
+          int64_t id;
+          int64_t root;
+          uint8_t* dst;
+          {
+            std::lock_guard<std::mutex> lk(s->mu);
+            id = s->pending[(size_t)g].front();
+            s->pending[(size_t)g].pop_front();
+            const Query& q = s->queries[id];
+            root = q.root;
+            dst = q.levels_out;
+          }
+          pw->t_start_us = s->now_us();
+          const int st = g500::bfs_launch_levels(pw->bfs, root, dst);
+          if (st != G500_OK) {
+            const std::vector<int64_t> ids{id};
+            finish_queries(s, ids, st, nullptr, nullptr, pw->t_start_us, 1, 0);
+            continue;
+          }
+          pw->busy = true;
+          pw->qid = id;
+          s->inflight_blocks += pw->units;
+          s->launches.fetch_add(1);
+          s->lanes_used.fetch_add(1);
+          const int f = s->in_flight.fetch_add(1) + 1;
+          int m = s->max_in_flight.load();
+          while (f > m && !s->max_in_flight.compare_exchange_weak(m, f)) {
+          }
+          any = true;
+          continue;
+        }
+        break;  // the plain worker is busy or the budget is full: wait for it
       }
       if (s->inflight_blocks + s->blocks[(size_t)g] > s->capacity) break;
       Worker* w = nullptr;
@@ -352,6 +429,38 @@ int submit_at(g500_server* s, int graph, int64_t root, uint64_t tag, uint8_t* le
   return G500_OK;
 }
 
+// plain_below for graph g: the given value, or (negative) the number of
+// queries whose one-at-a-time plain runs cost what one multi-source launch of
+// a single root costs, both timed here on a few roots (at most 32).
+int calibrate_plain(g500_server* s, int g, int given) {
+  if (given >= 0) {
+    s->plain_below[(size_t)g] = given;
+    return G500_OK;
+  }
+  g500_graph* gr = s->graphs[(size_t)g];
+  int64_t roots[4];
+  int found = 0;
+  G500_TRY(g500_graph_find_roots(gr, 4, 2, 3, roots, &found));
+  if (found == 0) return G500_OK;
+  g500_bfs* b = s->pworkers[(size_t)g][0].bfs;
+  g500_msbfs* m = s->workers[(size_t)g][0].ms;
+  G500_TRY(g500_msbfs_set_params(m, 32, s->alpha[(size_t)g], 1));
+  double tp = 1e300, tm = 1e300;
+  for (int rep = 0; rep < 3; ++rep)
+    for (int i = 0; i < found; ++i) {
+      const auto t0 = clk::now();
+      G500_TRY(g500::bfs_launch_levels(b, roots[i], nullptr));
+      G500_TRY(g500::bfs_complete(b, nullptr, nullptr));
+      tp = std::min(tp, std::chrono::duration<double>(clk::now() - t0).count());
+      g500_msbfs_stats st;
+      const auto t1 = clk::now();
+      G500_TRY(g500_msbfs_run(m, &roots[i], 1, nullptr, 0, &st));
+      tm = std::min(tm, std::chrono::duration<double>(clk::now() - t1).count());
+    }
+  s->plain_below[(size_t)g] = (int)std::max(0.0, std::min(32.0, std::floor(tm / tp)));
+  return G500_OK;
+}
+
 }  // namespace
 
 extern "C" int g500_server_default_config(g500_server_config* cfg) {
@@ -364,6 +473,7 @@ extern "C" int g500_server_default_config(g500_server_config* cfg) {
   cfg->hbm_reserve_bytes = 1ull << 30;
   cfg->alpha = 6.0;
   cfg->max_grid_fraction = 0.5;
+  cfg->plain_below = -1;
   return G500_OK;
 }
 
@@ -390,6 +500,9 @@ extern "C" int g500_server_create(g500_graph* const* graphs, int num_graphs, con
   s->t0 = clk::now();
   s->pending.resize((size_t)num_graphs);
   s->workers.resize((size_t)num_graphs);
+  s->pworkers.resize((size_t)num_graphs);
+  s->plain_below.assign((size_t)num_graphs, 0);
+  s->pblocks.assign((size_t)num_graphs, 0);
   s->blocks.assign((size_t)num_graphs, 0);
   s->alpha.assign((size_t)num_graphs, c.alpha);
   s->ws_bytes.assign((size_t)num_graphs, 0);
@@ -419,6 +532,19 @@ extern "C" int g500_server_create(g500_graph* const* graphs, int num_graphs, con
         w.blocks = s->blocks[(size_t)g];
         s->workers[(size_t)g].push_back(std::move(w));
         s->nworkers.fetch_add(1);
+      }
+      // one plain handle per graph, on the same share of the device
+      if (st == G500_OK && c.plain_below != 0) {
+        PlainWorker pw;
+        st = g500_bfs_create(graphs[g], &pw.bfs);
+        if (st == G500_OK) {
+          const int pb = std::max(1, s->blocks[(size_t)g] / 2);  // 512-thread blocks
+          st = g500_bfs_set_grid(pw.bfs, pb);
+          pw.units = 2 * pb;
+          s->pblocks[(size_t)g] = pb;
+        }
+        if (pw.bfs) s->pworkers[(size_t)g].push_back(pw);
+        if (st == G500_OK) st = calibrate_plain(s, g, c.plain_below);
       }
     }
   } else {
@@ -595,6 +721,11 @@ extern "C" int g500_server_destroy(g500_server* s) {
         g500_msbfs_wait(w.ms, nullptr);
       }
       g500_msbfs_destroy(w.ms);
+    }
+  for (auto& ps : s->pworkers)
+    for (PlainWorker& w : ps) {
+      if (w.busy) g500::bfs_complete(w.bfs, nullptr, nullptr);
+      g500_bfs_destroy(w.bfs);
     }
   for (g500_bfs* b : s->plain)
     if (b) g500_bfs_destroy(b);

@@ -172,6 +172,9 @@ int g500_bfs_set_stream(g500_bfs* b, void* stream);
  * discovered, 2 deferred: entries by reordered id during the search, then one
  * sequential pass in original-id order.  Results are identical. */
 int g500_bfs_set_pred_mode(g500_bfs* b, int mode);
+/* Blocks of the persistent kernel (0 = every co-resident block of the device);
+ * fewer leave SMs to kernels of other handles running at the same time. */
+int g500_bfs_set_grid(g500_bfs* b, int blocks);
 
 /* Autotuner: time every (policy, alpha, beta) of a built-in grid on the given
  * roots (device pred, best of `reps` runs per root), keep the fastest on the
@@ -313,6 +316,9 @@ typedef struct g500_server_config {
   double alpha;                  /* multi-source direction threshold (g500_msbfs_set_params) */
   double max_grid_fraction;      /* a launch uses at most this share of the device's co-resident blocks
                                     (so that launches of other graphs run beside it); (0, 1] */
+  int32_t plain_below;           /* a graph with at most this many waiting queries runs them one plain
+                                    BFS each (0 never; negative: calibrated per graph at create) */
+  int32_t pad;
 } g500_server_config;
 
 typedef struct g500_query_result {

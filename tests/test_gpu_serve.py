@@ -66,7 +66,8 @@ def run_alone(g500, graphs, queries, **cfg):
     return out
 
 
-def test_serve_levels_alone_and_in_mix(g500, served):
+@pytest.mark.parametrize("plain_below", [-1, 0, 1000])  # calibrated, never plain, always plain
+def test_serve_levels_alone_and_in_mix(g500, served, plain_below):
     graphs, oracles, _ = served
     alone_q = pick_queries(graphs, 9, seed=1)
     alone = run_alone(g500, graphs, alone_q)
@@ -77,7 +78,7 @@ def test_serve_levels_alone_and_in_mix(g500, served):
 
     # the mix: every alone query again, plus many more on every graph, submitted back to back
     mix_q = alone_q + pick_queries(graphs, 400, seed=2) + alone_q
-    srv = g500.Server(graphs, max_batch=128, max_workers_per_graph=2)
+    srv = g500.Server(graphs, max_batch=128, max_workers_per_graph=2, plain_below=plain_below)
     bufs, ids = [], []
     for gi, r in mix_q:
         b = np.full(graphs[gi].pred_size(), 7, np.uint8)
@@ -94,8 +95,11 @@ def test_serve_levels_alone_and_in_mix(g500, served):
     assert len(results) == len(mix_q)
     info = srv.info()
     srv.close()
-    assert info["launches"] < len(mix_q), "queries were not batched"
-    assert max(x["batch_size"] for x in results.values()) > 1
+    if plain_below == 0:
+        assert info["launches"] < len(mix_q), "queries were not batched"
+        assert max(x["batch_size"] for x in results.values()) > 1
+    if plain_below == 1000:
+        assert all(x["batch_size"] == 1 and x["lane_width"] == 0 for x in results.values())
     for k, (gi, r) in enumerate(mix_q):
         res = results[ids[k]]
         assert res["status"] == 0 and res["tag"] == k and res["graph"] == gi and res["root"] == r
