@@ -426,7 +426,8 @@ class BfsOnGPU:
             check(lib().g500_bfs_set_policy(self.h, policy))
 
     def set_pred_mode(self, mode: int = 0) -> None:
-        """0 by pred size, 1 pred written as vertices are found, 2 deferred (one pass at the end)."""
+        """0 by pred size, 1 pred written as vertices are found, 2 deferred (one pass at the end),
+        3 deferred with 32-bit entries (a search deeper than 31 levels reruns in mode 2)."""
         check(lib().g500_bfs_set_pred_mode(self.h, mode))
 
     def autotune(self, roots, reps: int = 2) -> dict:

@@ -13,8 +13,9 @@
 //   pred      int64 per ORIGINAL id: parent | level << 48 (bfs.hpp:1203,
 //             :2470), root = root (:498), -1 unreached.  Written as vertices
 //             are found, or (deferred mode, for pred arrays beyond L2) by
-//             reordered id into pred_r during the search and in original-id
-//             order by one sequential pass at the end
+//             reordered id into pred_r during the search (packed in 32 bits
+//             where the ids allow) and in original-id order by one sequential
+//             pass after it (deferred_pred_kernel)
 //
 // Top-down (top_down_search, bfs.hpp:1139-1166, :1249-1364): a warp takes B
 // work items (B adapts to the queue length so every warp has work), prefix-
@@ -48,6 +49,14 @@ constexpr int BFS_THREADS = 512;
 // pred at random during the search costs a DRAM read-modify-write per
 // discovered vertex once pred no longer fits in L2.
 constexpr uint64_t BFS_DEFERRED_PRED_BYTES = 100ull << 20;
+// Packed deferred entries: parent original id in the low PACK_SHIFT bits, the
+// level above it, in 32 bits instead of 64.  At SCALE 26 that halves the
+// array the final pass gathers from (131 MB against 262 MB), so most of the
+// gathers hit L2.  Graphs with more than 2^PACK_SHIFT vertex ids use 64-bit
+// entries; a search that reaches level PACK_LEVELS stops, and the host runs
+// it again with 64-bit entries (and keeps them for that handle).
+constexpr int PACK_SHIFT = 27;
+constexpr int PACK_LEVELS = 1 << (32 - PACK_SHIFT);
 constexpr int BFS_MIN_BLOCKS = 2;        // co-resident blocks per SM (64 registers, no spills)
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
 constexpr int BU_WORDS = 8;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
@@ -62,7 +71,9 @@ struct RunParams {
   const uint32_t* __restrict__ vis_init;
   int64_t* __restrict__ pred;
   int64_t* __restrict__ pred_r;  // deferred mode: pred entries by reordered id, [nlv]
-  int deferred;                  // write pred_r during the search, pred in one pass at the end
+  uint32_t* pred_p;              // the same buffer holding packed entries (deferred == 2)
+  int deferred;                  // 0: pred as found; 1: pred_r during the search, pred in one pass
+                                 // at the end; 2: the same with packed entries
   uint32_t first_id;             // mask of the vertex id in first[] (FIRST_ID, or all bits without flags)
   uint32_t first_more;           // FIRST_MORE, or 0 when first[] has no flags (every miss is scanned)
   uint32_t* vis[2];
@@ -77,6 +88,24 @@ struct RunParams {
 };
 
 constexpr uint32_t FIRST_CHUNK = 0x80000000u;
+
+// deferred modes (DEF = RunParams::deferred, a template argument of the
+// kernel so that each mode compiles to its own code): the entry of reordered
+// vertex r (parent's original id, level << 48)
+template <int DEF>
+__device__ __forceinline__ void put_deferred(const RunParams& p, int64_t r, uint32_t parent, int64_t lvl) {
+  if constexpr (DEF == 2) p.pred_p[r] = parent | ((uint32_t)(lvl >> 48) << PACK_SHIFT);
+  else p.pred_r[r] = (int64_t)parent | lvl;
+}
+
+template <int DEF>
+__device__ __forceinline__ int64_t get_deferred(const RunParams& p, int64_t r) {
+  if constexpr (DEF == 2) {
+    const uint32_t e = __ldcg(p.pred_p + r);
+    return (int64_t)(e & ((1u << PACK_SHIFT) - 1u)) | ((int64_t)(e >> PACK_SHIFT) << 48);
+  }
+  return __ldcg(p.pred_r + r);
+}
 
 __device__ __forceinline__ uint32_t chunks_of(uint64_t deg) { return (uint32_t)((deg + TD_CHUNK - 1) / TD_CHUNK); }
 
@@ -126,6 +155,7 @@ __device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t o
 // Top-down level: expand the work items, claim unvisited targets, and list the
 // discovered (vertex, original id) pairs.  Rows are cut into work items only
 // if the next level is top-down as well (chunk_phase).
+template <int DEF>
 __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, int64_t qn, uint32_t* vis,
                          uint2* __restrict__ found_list, unsigned long long* cnt, unsigned long long* sh_acc,
                          int64_t lvl) {
@@ -180,7 +210,7 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
         ow[j] = 0;
         if (won[j]) {
           ow[j] = __ldg(p.invert + w[j]);
-          if (p.deferred) p.pred_r[w[j]] = (int64_t)uo[j] | lvl;
+          if constexpr (DEF != 0) put_deferred<DEF>(p, w[j], uo[j], lvl);
           else p.pred[ow[j]] = (int64_t)uo[j] | lvl;
           if (p.policy == G500_DIR_EDGES) mf += __ldg(p.off + w[j] + 1) - __ldg(p.off + w[j]);
         }
@@ -245,6 +275,7 @@ __device__ __forceinline__ bool vis_test(const uint32_t* __restrict__ vis, uint3
 //  B. the warp gathers 32 misses of its words into its lanes (select_bit); a
 //     lane checks BU_SERIAL more row entries alone, and rows still unresolved
 //     are scanned by the whole warp.
+template <int DEF>
 __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint32_t* __restrict__ vis_next,
                          unsigned long long* sh_acc, int64_t lvl) {
   const int lane = threadIdx.x & 31;
@@ -292,9 +323,9 @@ __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cu
         }
         if (hit) {
           const int64_t vr = (int64_t)wj[u] * 32 + lane;
-          const int64_t val = (int64_t)__ldg(p.invert + fv) | lvl;
-          if (p.deferred) p.pred_r[vr] = val;
-          else p.pred[__ldg(p.invert + vr)] = val;
+          const uint32_t par = __ldg(p.invert + fv);
+          if constexpr (DEF != 0) put_deferred<DEF>(p, vr, par, lvl);
+          else p.pred[__ldg(p.invert + vr)] = (int64_t)par | lvl;
         }
       }
     }
@@ -367,9 +398,9 @@ __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cu
       }
       if (parent != NO_VERTEX) {
         atomicOr(vis_next + (v >> 5), 1u << (v & 31));
-        const int64_t val = (int64_t)__ldg(p.invert + parent) | lvl;
-        if (p.deferred) p.pred_r[v] = val;
-        else p.pred[__ldg(p.invert + v)] = val;
+        const uint32_t par = __ldg(p.invert + parent);
+        if constexpr (DEF != 0) put_deferred<DEF>(p, v, par, lvl);
+        else p.pred[__ldg(p.invert + v)] = (int64_t)par | lvl;
         ++found_b;
       }
       if (p.count_edges && v != NO_VERTEX) {
@@ -434,6 +465,7 @@ __device__ __forceinline__ void write_record(LevelRecord* rec, int level, bool t
   rec[level - 1] = r;
 }
 
+template <int DEF>
 __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_kernel(RunParams p) {
   __shared__ unsigned long long sh_cnt[C_NUM];
   __shared__ unsigned long long sh_acc[C_NUM];
@@ -455,9 +487,10 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   const uint64_t root_b = has_edges ? p.off[root_r] : 0;
   const uint64_t root_deg = has_edges ? p.off[root_r + 1] - root_b : 0;
   const int64_t root_items = (int64_t)chunks_of(root_deg);
-  if (!p.deferred || !has_edges)  // deferred mode writes pred whole at the end
+  if (DEF == 0 || !has_edges)  // deferred mode writes pred whole at the end
     for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = i == p.root ? p.root : -1;
-  if (p.deferred && has_edges && tid == 0) p.pred_r[root_r] = p.root;
+  if constexpr (DEF != 0)
+    if (has_edges && tid == 0) put_deferred<DEF>(p, root_r, (uint32_t)p.root, 0);
   for (int64_t i = tid; i < p.nwords; i += nthreads)
     p.vis[0][i] = p.vis_init[i] | (has_edges && i == (int64_t)(root_r >> 5) ? 1u << (root_r & 31) : 0u);
   if (blockIdx.x == 0 && threadIdx.x < 3 * C_NUM) (&ctl->cnt[0][0])[threadIdx.x] = 0;
@@ -496,11 +529,15 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   (blockIdx.x == 0 && threadIdx.x < C_NUM ? (void)(ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0) : (void)0), \
       ctl->cnt[phase % 3]
   for (;; ++level) {
+    if (DEF == 2 && level >= PACK_LEVELS) {  // the packed level field is full: the host reruns unpacked
+      if (tid == 0) atomicOr(&ctl->bar.err, (unsigned)BFS_ERR_PACK);
+      return;
+    }
     unsigned long long* cnt = (NEXT_PHASE_SLOT());
     const int64_t lvl = (int64_t)level << 48;
     unsigned long long disc, scan = 0, edges, sect, front = 0, listed = 0, t_mid = 0, mf = 0;
     if (forward) {
-      td_phase(p, items, qn, p.vis[cur_vis], found_list, cnt, sh_acc, lvl);
+      td_phase<DEF>(p, items, qn, p.vis[cur_vis], found_list, cnt, sh_acc, lvl);
       if (!grid_sync<C_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
       if (tid == 0) t_mid = globaltimer();
       ++phase;
@@ -511,7 +548,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       listed = sh_cnt[C_QITEMS];
       mf = sh_cnt[C_MF];
     } else {
-      bu_level(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], sh_acc, lvl);
+      bu_level<DEF>(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], sh_acc, lvl);
       if (!grid_sync<C_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
       if (tid == 0) t_mid = globaltimer();
       ++phase;
@@ -568,45 +605,55 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
                    edges + (was_forward ? carried_in : 0), sect + (was_forward ? carried_in : 0), t_mid);
   }
 #undef NEXT_PHASE_SLOT
-  if (p.deferred) {
-    // pred in original-id order, sequential writes: a reached vertex (visited
-    // now, not pre-visited for lack of edges) takes its entry from pred_r.
-    // 8 consecutive vertices per thread, all loads of a step issued together;
-    // the streamed map and pred bypass L2 retention (evict-first), so that the
-    // gathered bitmaps and pred_r stay cached.  nolv is a multiple of 65536.
-    const uint32_t* vf = p.vis[cur_vis];
-    if (reinterpret_cast<uintptr_t>(p.pred) & 15) {  // a caller's pred not 16-byte aligned: one entry at a time
-      for (int64_t u = tid; u < p.nolv; u += nthreads) {
-        const uint32_t r = __ldg(p.reorder + u);
-        int64_t val = -1;
-        if ((int64_t)r < p.nlv && (((__ldcg(vf + (r >> 5)) & ~__ldg(p.vis_init + (r >> 5))) >> (r & 31)) & 1u))
-          val = __ldcg(p.pred_r + r);
-        p.pred[u] = val;
-      }
-    } else
-    for (int64_t u0 = tid * 8; u0 < p.nolv; u0 += nthreads * 8) {
-      const uint4 ra = __ldcs(reinterpret_cast<const uint4*>(p.reorder + u0));
-      const uint4 rb = __ldcs(reinterpret_cast<const uint4*>(p.reorder + u0 + 4));
-      const uint32_t r[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
-      bool reach[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        reach[i] = false;
-        if ((int64_t)r[i] < p.nlv)
-          reach[i] = ((__ldcg(vf + (r[i] >> 5)) & ~__ldg(p.vis_init + (r[i] >> 5))) >> (r[i] & 31)) & 1u;
-      }
-      long long val[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) val[i] = reach[i] ? (long long)__ldcg(p.pred_r + r[i]) : -1ll;
-      longlong2* dst = reinterpret_cast<longlong2*>(p.pred + u0);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) __stcs(dst + i, make_longlong2(val[2 * i], val[2 * i + 1]));
-    }
-  }
   if (tid == 0) {
     ctl->num_levels = (unsigned)level;
     ctl->final_vis = cur_vis;
     ctl->t_end_ns = globaltimer();
+  }
+}
+
+// Deferred modes, after the search: pred in original-id order with
+// sequential writes.  A reached vertex (visited now, not pre-visited for lack
+// of edges) takes its entry from pred_r.  Its own launch, so that 2048 threads
+// per SM (the persistent kernel has 1024) keep the gathers in flight; 4
+// consecutive vertices per thread, every load of a thread issued together
+// (an unreached vertex's entry is stale and dropped).  The streamed map and
+// pred are evict-first, so that the gathered bitmaps and entries stay in L2.
+// nolv is a multiple of 65536.
+constexpr int FINAL_THREADS = 256;
+template <int DEF>
+__global__ void __launch_bounds__(FINAL_THREADS, 8) deferred_pred_kernel(RunParams p) {
+  const BfsCtl* ctl = p.ctl;
+  if (!ctl->root_has_edges || ctl->bar.err) return;  // pred already written, or the search failed
+  const uint32_t* vf = p.vis[ctl->final_vis];
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  if (reinterpret_cast<uintptr_t>(p.pred) & 15) {  // a caller's pred not 16-byte aligned: one entry at a time
+    for (int64_t u = tid; u < p.nolv; u += nthreads) {
+      const uint32_t r = __ldg(p.reorder + u);
+      int64_t val = -1;
+      if ((int64_t)r < p.nlv && (((__ldcg(vf + (r >> 5)) & ~__ldg(p.vis_init + (r >> 5))) >> (r & 31)) & 1u))
+        val = get_deferred<DEF>(p, r);
+      p.pred[u] = val;
+    }
+    return;
+  }
+  for (int64_t u0 = tid * 4; u0 < p.nolv; u0 += nthreads * 4) {
+    const uint4 ra = __ldcs(reinterpret_cast<const uint4*>(p.reorder + u0));
+    const uint32_t r[4] = {ra.x, ra.y, ra.z, ra.w};
+    long long val[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      val[i] = -1ll;
+      if ((int64_t)r[i] < p.nlv) {
+        const uint32_t wv = __ldcg(vf + (r[i] >> 5)), wi = __ldg(p.vis_init + (r[i] >> 5));
+        const long long e = (long long)get_deferred<DEF>(p, r[i]);
+        if (((wv & ~wi) >> (r[i] & 31)) & 1u) val[i] = e;
+      }
+    }
+    longlong2* dst = reinterpret_cast<longlong2*>(p.pred + u0);
+    __stcs(dst, make_longlong2(val[0], val[1]));
+    __stcs(dst + 1, make_longlong2(val[2], val[3]));
   }
 }
 
@@ -660,6 +707,22 @@ static int bfs_free(g500_bfs* b) {
   return G500_OK;
 }
 
+// the deferred modes' final pass, enqueued right after the search
+static int launch_deferred_pred(const RunParams& p, cudaStream_t s) {
+  if (!p.deferred) return G500_OK;
+  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(p.nolv / 4, FINAL_THREADS), (int64_t)num_sms() * 64);
+  if (p.deferred == 2) deferred_pred_kernel<2><<<grid, FINAL_THREADS, 0, s>>>(p);
+  else deferred_pred_kernel<1><<<grid, FINAL_THREADS, 0, s>>>(p);
+  G500_CUDA(cudaGetLastError());
+  return G500_OK;
+}
+
+static const void* bfs_kernel_for(int deferred) {
+  if (deferred == 2) return (const void*)bfs_persistent_kernel<2>;
+  if (deferred == 1) return (const void*)bfs_persistent_kernel<1>;
+  return (const void*)bfs_persistent_kernel<0>;
+}
+
 // The kernel's parameters for one run from `root` writing pred to `pred`.
 static int make_params(g500_bfs* b, int64_t root, int64_t* pred, RunParams* out) {
   g500_graph* g = b->g;
@@ -673,9 +736,13 @@ static int make_params(g500_bfs* b, int64_t root, int64_t* pred, RunParams* out)
   p.reorder = g->d_reorder;
   p.vis_init = g->d_vis_init;
   p.pred = pred;
-  p.deferred = b->pred_mode == 2 || (b->pred_mode == 0 && (uint64_t)g->nolv * 8 > BFS_DEFERRED_PRED_BYTES);
+  int mode = b->pred_mode;
+  if (mode == 0) mode = (uint64_t)g->nolv * 8 > BFS_DEFERRED_PRED_BYTES ? 3 : 1;
+  if (mode == 3 && (b->pack_off || g->nolv > (1ll << PACK_SHIFT))) mode = 2;
+  p.deferred = mode == 1 ? 0 : (mode == 2 ? 1 : 2);
   if (p.deferred && !b->d_pred_r) G500_TRY(dev_alloc_n(&b->d_pred_r, std::max<int64_t>(g->nlv, 1), "deferred pred"));
   p.pred_r = b->d_pred_r;
+  p.pred_p = reinterpret_cast<uint32_t*>(b->d_pred_r);
   p.vis[0] = b->d_vis[0];
   p.vis[1] = b->d_vis[1];
   p.queue[0] = b->d_queue[0];
@@ -737,7 +804,7 @@ extern "C" int g500_bfs_create(g500_graph* g, g500_bfs** out) {
   chk(cudaEventCreate(&b->ev1), "cudaEventCreate");
   if (st == G500_OK) {
     int per_sm = 0;
-    chk(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_persistent_kernel, BFS_THREADS, 0),
+    chk(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_persistent_kernel<2>, BFS_THREADS, 0),
         "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     int coop = 0;
     chk(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, g->device), "cudaDeviceGetAttribute");
@@ -779,8 +846,9 @@ int bfs_launch_levels(g500_bfs* b, int64_t root, uint8_t* levels_dst) {
   void* args[] = {&p};
   G500_CUDA(cudaMemsetAsync(b->d_ctl, 0, sizeof(BfsCtl), s));
   G500_CUDA(cudaMemsetAsync(b->d_overflow, 0, sizeof(unsigned), s));
-  G500_CUDA(cudaLaunchCooperativeKernel((const void*)bfs_persistent_kernel, dim3(b->grid), dim3(BFS_THREADS), args,
+  G500_CUDA(cudaLaunchCooperativeKernel(bfs_kernel_for(p.deferred), dim3(b->grid), dim3(BFS_THREADS), args,
                                         0, s));
+  G500_TRY(launch_deferred_pred(p, s));
   const unsigned rg = (unsigned)std::min<int64_t>(ceil_div(std::max<int64_t>(p.nwords, 1), 256), num_sms() * 8);
   reach_kernel<<<rg, 256, 0, s>>>(b->d_vis[0], b->d_vis[1], g->d_vis_init, g->d_endp, p.nwords, b->d_ctl);
   const unsigned lg = (unsigned)std::min<int64_t>(ceil_div(g->nolv, 256), num_sms() * 8);
@@ -791,6 +859,7 @@ int bfs_launch_levels(g500_bfs* b, int64_t root, uint8_t* levels_dst) {
   G500_CUDA(cudaMemcpyAsync(&b->h_ctl->pad_overflow, b->d_overflow, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   G500_CUDA(cudaEventRecord(b->ev_done, s));
   b->last_root = root;
+  b->last_levels_dst = levels_dst;
   b->in_flight = 1;
   return G500_OK;
 }
@@ -819,6 +888,11 @@ int bfs_complete(g500_bfs* b, int64_t* reached, int64_t* nedge) {
   if (e != cudaSuccess) return cuda_error(e, "cudaEventSynchronize", __FILE__, __LINE__);
   const BfsCtl& c = *b->h_ctl;
   if (c.bar.err & BFS_ERR_TIMEOUT) return set_error(G500_E_TIMEOUT, "grid barrier wait gave up (bounded spin)");
+  if (c.bar.err & BFS_ERR_PACK) {  // deeper than the packed entries hold: the same run with 64-bit entries
+    b->pack_off = 1;
+    G500_TRY(bfs_launch_levels(b, b->last_root, b->last_levels_dst));
+    return bfs_complete(b, reached, nedge);
+  }
   if (c.bar.err & BFS_ERR_QUEUE) return set_error(G500_E_RANGE, "top-down queue overflow");
   if (c.bar.err & BFS_ERR_DEPTH) return set_error(G500_E_RANGE, "BFS depth exceeds the 16-bit level field");
   if (c.pad_overflow) return set_error(G500_E_RANGE, "a level over 254 does not fit the uint8 levels");
@@ -848,7 +922,7 @@ extern "C" int g500_bfs_set_params(g500_bfs* b, double alpha, double beta, int c
 
 extern "C" int g500_bfs_set_pred_mode(g500_bfs* b, int mode) {
   if (!b) return set_error(G500_E_INVAL, "null bfs");
-  if (mode < 0 || mode > 2) return set_error(G500_E_INVAL, "unknown pred mode %d", mode);
+  if (mode < 0 || mode > 3) return set_error(G500_E_INVAL, "unknown pred mode %d", mode);
   b->pred_mode = mode;
   return G500_OK;
 }
@@ -937,8 +1011,9 @@ extern "C" int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_o
   void* args[] = {&p};
   G500_CUDA(cudaMemsetAsync(b->d_ctl, 0, sizeof(BfsCtl), s));
   G500_CUDA(cudaEventRecord(b->ev0, s));
-  G500_CUDA(cudaLaunchCooperativeKernel((const void*)bfs_persistent_kernel, dim3(b->grid), dim3(BFS_THREADS), args,
+  G500_CUDA(cudaLaunchCooperativeKernel(bfs_kernel_for(p.deferred), dim3(b->grid), dim3(BFS_THREADS), args,
                                         0, s));
+  G500_TRY(launch_deferred_pred(p, s));
   G500_CUDA(cudaEventRecord(b->ev1, s));
   if (stats) {
     const unsigned rg = (unsigned)std::min<int64_t>(ceil_div(std::max<int64_t>(p.nwords, 1), 256), num_sms() * 8);
@@ -952,6 +1027,10 @@ extern "C" int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_o
   b->last_root = root;
   const BfsCtl& c = *b->h_ctl;
   if (c.bar.err & BFS_ERR_TIMEOUT) return set_error(G500_E_TIMEOUT, "grid barrier wait gave up (bounded spin)");
+  if (c.bar.err & BFS_ERR_PACK) {  // deeper than the packed entries hold: the same run with 64-bit entries
+    b->pack_off = 1;
+    return g500_bfs_run(b, root, pred, pred_on_device, stats);
+  }
   if (c.bar.err & BFS_ERR_QUEUE) return set_error(G500_E_RANGE, "top-down queue overflow");
   if (c.bar.err & BFS_ERR_DEPTH) return set_error(G500_E_RANGE, "BFS depth exceeds the 16-bit level field");
   if (stats) {
@@ -971,7 +1050,7 @@ extern "C" int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_o
       stats->nedge = e / 2;
     }
     stats->num_levels = (int32_t)c.num_levels;
-    stats->kernel_launches = 1;
+    stats->kernel_launches = p.deferred ? 2 : 1;
     if (c.t_init_ns >= c.t0_ns) stats->init_ms = (double)(c.t_init_ns - c.t0_ns) * 1e-6;
     if (c.t_end_ns >= c.t_init_ns) stats->search_ms = (double)(c.t_end_ns - c.t_init_ns) * 1e-6;
     if (c.num_levels) {

@@ -126,7 +126,7 @@ struct __align__(16) TdItem {
   uint32_t orig;             // original id of the row's vertex (the parent written to pred)
   uint32_t len;              // chunk length; bit 31 marks the row's first chunk
 };
-enum BfsErr { BFS_ERR_QUEUE = 1, BFS_ERR_TIMEOUT = 2, BFS_ERR_DEPTH = 4 };
+enum BfsErr { BFS_ERR_QUEUE = 1, BFS_ERR_TIMEOUT = 2, BFS_ERR_DEPTH = 4, BFS_ERR_PACK = 8 };
 constexpr unsigned GRID_ERR_TIMEOUT = 2;  // same bit as BFS_ERR_TIMEOUT
 
 // State of a grid-wide barrier of a cooperative kernel (device memory, zeroed
@@ -179,7 +179,9 @@ struct g500_bfs {
   cudaEvent_t ev_done = nullptr;
   int in_flight = 0;
   unsigned grid_full = 0;            // every co-resident block of the device
-  int pred_mode = 0;                 // 0 by pred size, 1 direct, 2 deferred
+  int pred_mode = 0;                 // 0 by pred size, 1 direct, 2 deferred, 3 deferred packed
+  int pack_off = 0;                  // a search outgrew the packed level field: deferred runs stay unpacked
+  uint8_t* last_levels_dst = nullptr;  // levels destination of the run in flight (a rerun writes it again)
   uint32_t* d_vis[2] = {nullptr, nullptr};
   TdItem* d_queue[2] = {nullptr, nullptr};
   int64_t queue_cap = 0;

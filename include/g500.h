@@ -170,7 +170,9 @@ int g500_bfs_set_policy(g500_bfs* b, int policy);
 int g500_bfs_set_stream(g500_bfs* b, void* stream);
 /* How run writes pred: 0 (default) by its size, 1 at random as vertices are
  * discovered, 2 deferred: entries by reordered id during the search, then one
- * sequential pass in original-id order.  Results are identical. */
+ * sequential pass in original-id order, 3 deferred with 32-bit entries (graphs
+ * of at most 2^27 vertex ids; a search deeper than 31 levels is run again
+ * with mode 2, which the handle then keeps).  Results are identical. */
 int g500_bfs_set_pred_mode(g500_bfs* b, int mode);
 /* Blocks of the persistent kernel (0 = every co-resident block of the device);
  * fewer leave SMs to kernels of other handles running at the same time. */

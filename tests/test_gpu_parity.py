@@ -84,7 +84,7 @@ def test_graph_info_and_roots_match_reference(g500, scale, vr):
 
 
 # ----------------------------------------------------------------------- BFS
-@pytest.mark.parametrize("pred_mode", [1, 2])  # pred written as found / deferred to one final pass
+@pytest.mark.parametrize("pred_mode", [1, 2, 3])  # pred written as found / deferred to one final pass / packed
 @pytest.mark.parametrize("scale,vr", GOLDEN_CASES)
 def test_bfs_levels_and_validation(g500, oracle_mod, scale, vr, pred_mode):
     rec, arr = load_golden(scale, vr)
@@ -197,7 +197,7 @@ def _edges_from_pairs(g500, pairs):
     return a
 
 
-@pytest.mark.parametrize("pred_mode", [1, 2])
+@pytest.mark.parametrize("pred_mode", [1, 2, 3])  # 3 on the path graph: deeper than the packed field
 @pytest.mark.parametrize("name", ["path", "star", "two_components", "self_loops_dups", "high_ids", "isolated_root"])
 @pytest.mark.parametrize("vr", [0, 1, 2])
 def test_small_graphs(g500, oracle_mod, name, vr, pred_mode):
