@@ -117,26 +117,44 @@ class ClockSampler:
         self.gpu = gpu
         self.proc = None
         self.path = None
+        self.first = 0
+
+    def _lines(self) -> list:
+        with open(self.path) as f:
+            return [ln for ln in f.read().split("\n")[:-1] if ln.strip()]  # complete lines only
 
     def start(self):
+        """Start sampling every 50 ms and return once the first sample is in,
+        so that the timed region that follows is covered from its start."""
         if not shutil.which("nvidia-smi"):
             return
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                      "--format=csv,noheader,nounits", "-lms", "50"],
                                      stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        t_end = time.time() + 10.0
+        while time.time() < t_end and not self._lines() and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.first = len(self._lines())
 
     def stop(self) -> dict | None:
+        """The samples taken during the timed region; a region shorter than
+        the sampling interval gets the first sample after it instead."""
         if not self.proc:
             return None
+        last = len(self._lines())
+        t_end = time.time() + 1.0
+        while last == self.first and time.time() < t_end and self.proc.poll() is None:
+            time.sleep(0.01)
+            last = len(self._lines())
         self.proc.terminate()
         try:
             self.proc.wait(5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
         rows = []
-        for line in open(self.path):
+        for line in self._lines()[self.first:max(last, self.first + 1)]:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -155,7 +173,9 @@ class ClockSampler:
                 if r[k].lower().startswith("active"):
                     reasons.add(name)
         return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["max"] for r in rows),
-                "samples": len(rows), "reasons": sorted(reasons)}
+                "samples": len(rows), "sampled": "during the timed region" if last > self.first else
+                "first sample after the timed region (shorter than the 50 ms interval)",
+                "reasons": sorted(reasons)}
 
 
 # --------------------------------------------------------------------------- CPU baseline

@@ -136,7 +136,7 @@ __device__ __forceinline__ bool covers(const Mask<NW>& acc, const Mask<NW>& need
 
 constexpr int MS_WIN = 128;            // push: virtual edges a warp takes per window (4 per lane)
 constexpr int MS_GROUPS = 4;           // push: groups of 32 rows whose frontier masks load together
-constexpr int MS_SMALL_DEG = 64;       // pull: rows up to this long are walked by one thread
+constexpr int MS_SMALL_DEG = 128;      // pull: rows up to this long are walked by one thread
 constexpr int MS_UNROLL = 4;           // pull: neighbours each thread loads per step
 constexpr int MS_HUB_DEG = 1024;       // pull: rows longer than this are hub rows, split across warps
 constexpr int MS_HUB_CHUNK = 1024;     // pull: edges of a hub row one warp takes at a time

@@ -559,6 +559,19 @@ extern "C" int g500_server_create(g500_graph* const* graphs, int num_graphs, con
       if (e != cudaSuccess) st = g500::cuda_error(e, "plain-mode buffers", __FILE__, __LINE__);
     }
   }
+  // The other workers are created now, round robin over the graphs, as many
+  // as free HBM admits: creating one inside the loop allocates and builds its
+  // hub tables on a busy device, which held every waiting query for 0.1-0.5 s.
+  if (st == G500_OK && c.mode == G500_SERVE_BATCHED)
+    for (int k = 1; k < c.max_workers_per_graph && st == G500_OK; ++k)
+      for (int g = 0; g < num_graphs && st == G500_OK; ++g) {
+        if (s->no_more[(size_t)g]) continue;
+        Worker nw;
+        const int ws = new_worker(s, g, &nw);
+        if (ws == G500_E_NOMEM) s->no_more[(size_t)g] = 1;
+        else if (ws != G500_OK) st = ws;
+        else s->workers[(size_t)g].push_back(std::move(nw));
+      }
   if (st != G500_OK) {
     g500_server_destroy(s);
     return st;

@@ -301,8 +301,10 @@ int g500_msbfs_destroy(g500_msbfs* m);
 /* A request loop over several resident graphs: BFS queries (graph, root) are
  * admitted as they arrive, batched into multi-source launches while earlier
  * launches run (continuous batching), and overlap on the device on separate
- * streams.  A new launch slot (a g500_msbfs workspace) is created only while
- * the device keeps hbm_reserve_bytes free.  No counterpart in the reference,
+ * streams.  The launch slots (g500_msbfs workspaces, up to
+ * max_workers_per_graph per graph) are created with the server, each only
+ * while the device keeps hbm_reserve_bytes free; a graph with fewer slots
+ * gets another later only if memory allows then.  No counterpart in the reference,
  * which runs one root at a time (main.cc:105-160).  Each query's levels equal
  * the plain BFS's (pred >> 48) for its root, alone or in any mix.  The graphs
  * stay owned by the caller and must outlive the server. */
