@@ -508,6 +508,7 @@ def our_arm(a):
     barrier()
     e2e_max = reduce_max(e2e_t)
     e2e_value = e_all / e2e_max / 1e9
+    pred_bytes = 8  # a pinned pred: one DMA copy of the int64 entries
     g5.check(g5.lib().g500_host_free(hp))
 
     # batched multi-source BFS on the same graph and roots (one launch per 64 roots)
@@ -538,7 +539,8 @@ def our_arm(a):
                        **tuning),
         "harmonic_mean_gteps": hm,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * len(roots),
-                "d2h_bytes_per_step": 8 * info.pred_size * len(roots)},
+                "d2h_bytes_per_step": pred_bytes * info.pred_size * len(roots),
+                "path": "g500_bfs_run into a pinned host int64 pred (one DMA copy per root)"},
         "gpu_launches": rec["launches"],
         "roofline": {"bound": "hbm", "kernel": "bfs_persistent_kernel", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_per_bfs(a),

@@ -160,6 +160,7 @@ def lib() -> C.CDLL:
         "g500_bfs_set_params": ([P, C.c_double, C.c_double, i32], i32),
         "g500_bfs_set_stream": ([P, P], i32),
         "g500_bfs_set_pred_mode": ([P, i32], i32),
+        "g500_bfs_set_host_pack": ([P, i32], i32),
         "g500_bfs_set_grid": ([P, i32], i32),
         "g500_bfs_set_policy": ([P, i32], i32),
         "g500_bfs_autotune": ([P, P, i32, i32, C.POINTER(TuneResult)], i32),
@@ -429,6 +430,11 @@ class BfsOnGPU:
         """0 by pred size, 1 pred written as vertices are found, 2 deferred (one pass at the end),
         3 deferred with 32-bit entries (a search deeper than 31 levels reruns in mode 2)."""
         check(lib().g500_bfs_set_pred_mode(self.h, mode))
+
+    def set_host_pack(self, on: bool = True) -> None:
+        """A pageable host pred crosses PCIe as packed 32-bit entries expanded by host threads (default),
+        or always as int64; a pinned pred is always one int64 DMA copy."""
+        check(lib().g500_bfs_set_host_pack(self.h, int(on)))
 
     def autotune(self, roots, reps: int = 2) -> dict:
         """Pick the direction policy and thresholds on sample roots (kept on the handle)."""

@@ -688,6 +688,7 @@ static int bfs_free(g500_bfs* b) {
   if (!b) return G500_OK;
   cudaSetDevice(b->g->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  pred_expander_free(b);
   dev_free(b->d_pred);
   dev_free(b->d_pred_r);
   dev_free(b->d_levels);
@@ -927,6 +928,12 @@ extern "C" int g500_bfs_set_pred_mode(g500_bfs* b, int mode) {
   return G500_OK;
 }
 
+extern "C" int g500_bfs_set_host_pack(g500_bfs* b, int on) {
+  if (!b) return set_error(G500_E_INVAL, "null bfs");
+  b->pack_host_off = on ? 0 : 1;
+  return G500_OK;
+}
+
 extern "C" int g500_bfs_set_policy(g500_bfs* b, int policy) {
   if (!b) return set_error(G500_E_INVAL, "null bfs");
   if (policy != G500_DIR_REFERENCE && policy != G500_DIR_EDGES)
@@ -1020,9 +1027,12 @@ extern "C" int g500_bfs_run(g500_bfs* b, int64_t root, int64_t* pred, int pred_o
     reach_kernel<<<rg, 256, 0, s>>>(b->d_vis[0], b->d_vis[1], g->d_vis_init, g->d_endp, p.nwords, b->d_ctl);
     G500_CUDA(cudaGetLastError());
   }
-  if (!pred_on_device)
-    G500_CUDA(cudaMemcpyAsync(pred, b->d_pred, sizeof(int64_t) * g->nolv, cudaMemcpyDeviceToHost, s));
   G500_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s));
+  if (!pred_on_device) {
+    bool packed = false;
+    G500_TRY(pred_to_host_packed(b, pred, s, &packed));
+    if (!packed) G500_CUDA(cudaMemcpyAsync(pred, b->d_pred, sizeof(int64_t) * g->nolv, cudaMemcpyDeviceToHost, s));
+  }
   G500_CUDA(cudaStreamSynchronize(s));
   b->last_root = root;
   const BfsCtl& c = *b->h_ctl;

@@ -163,6 +163,10 @@ struct LevelRecord {
 
 constexpr int MAX_LEVELS = 0xFFFE;
 
+namespace g500 {
+class PredExpander;
+}
+
 struct g500_bfs {
   g500_graph* g = nullptr;
   cudaStream_t own_stream = nullptr;
@@ -182,6 +186,13 @@ struct g500_bfs {
   int pred_mode = 0;                 // 0 by pred size, 1 direct, 2 deferred, 3 deferred packed
   int pack_off = 0;                  // a search outgrew the packed level field: deferred runs stay unpacked
   uint8_t* last_levels_dst = nullptr;  // levels destination of the run in flight (a rerun writes it again)
+  // a host pred crosses PCIe as packed 32-bit entries, expanded by host threads
+  int pack_host_off = 0;
+  uint32_t* d_pack = nullptr;        // [nolv]
+  unsigned* d_pack_ovf = nullptr;
+  uint32_t* h_pack = nullptr;        // pinned [nolv + 64]
+  cudaEvent_t ev_chunk[8] = {};
+  g500::PredExpander* expander = nullptr;
   uint32_t* d_vis[2] = {nullptr, nullptr};
   TdItem* d_queue[2] = {nullptr, nullptr};
   int64_t queue_cap = 0;
@@ -199,6 +210,13 @@ namespace g500 {
 int bfs_launch_levels(g500_bfs* b, int64_t root, uint8_t* levels_dst);
 int bfs_poll(g500_bfs* b, int* done);
 int bfs_complete(g500_bfs* b, int64_t* reached, int64_t* nedge);
+
+// Copy the run's pred (b->d_pred) to host_pred as packed entries, expanded by
+// host threads chunk by chunk; *packed = false when the graph or the run
+// does not fit the packed form (the caller then copies the int64 entries).
+// Enqueued on s after the run; returns when host_pred is complete.
+int pred_to_host_packed(g500_bfs* b, int64_t* host_pred, cudaStream_t s, bool* packed);
+void pred_expander_free(g500_bfs* b);
 
 // g500_msbfs_launch that also copies each root's level row (pred_size bytes)
 // to root_dsts[i] when it is not null, before the launch's completion event.

@@ -174,6 +174,15 @@ int g500_bfs_set_stream(g500_bfs* b, void* stream);
  * of at most 2^27 vertex ids; a search deeper than 31 levels is run again
  * with mode 2, which the handle then keeps).  Results are identical. */
 int g500_bfs_set_pred_mode(g500_bfs* b, int mode);
+/* A pageable host pred (g500_bfs_run with pred_on_device = 0, memory not
+ * pinned) crosses PCIe as 32-bit packed entries (parent id in 27 bits, level
+ * in 5) into pinned staging, in chunks that host threads expand into the
+ * caller's int64 array while the next chunk is copied: about twice as fast
+ * as the runtime's pageable copy.  A pinned pred gets one DMA copy of the
+ * int64 entries, as do graphs of more than 2^27 vertex ids and runs deeper
+ * than 30 levels.  on = 1 (default) or 0 (always copy the int64 entries);
+ * the values are the same. */
+int g500_bfs_set_host_pack(g500_bfs* b, int on);
 /* Blocks of the persistent kernel (0 = every co-resident block of the device);
  * fewer leave SMs to kernels of other handles running at the same time. */
 int g500_bfs_set_grid(g500_bfs* b, int blocks);

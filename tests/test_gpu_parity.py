@@ -190,6 +190,39 @@ def test_pred_in_device_memory(g500, oracle_mod):
     bfs.close()
 
 
+@pytest.mark.parametrize("scale,vr", [(16, 0), (18, 2)])
+def test_host_pred_transfers(g500, oracle_mod, scale, vr):
+    """A pageable host pred crosses PCIe as packed 32-bit entries that host
+    threads expand; a pinned one, or any with packing off, as int64.  Every
+    entry must be written (the buffer starts as garbage), the levels must be
+    the reference's and the parents must validate.  (Parents are compared by
+    validation, not entry by entry: two runs may pick different valid ones.)"""
+    import ctypes
+    rec, _ = load_golden(scale, vr)
+    bfs = g500.BfsOnGPU(reorder_mode=vr)
+    bfs.construct(g500.EdgeList(None, scale, 16))
+    bfs.prepare_bfs()
+    n = bfs.graph_.pred_size()
+    hp = ctypes.c_void_p()
+    g500.check(g500.lib().g500_host_alloc(8 * n, ctypes.byref(hp)))
+    pinned = np.ctypeslib.as_array((ctypes.c_int64 * n).from_address(hp.value))
+    edges = oracle_mod.generate_edges(scale)
+    nglob = bfs.graph_.info.max_used_vertex + 1
+    for pr in rec["per_root"][:3]:
+        root = pr["root"]
+        for on, kind in ((True, "pageable"), (False, "pageable"), (True, "pinned")):
+            bfs.set_host_pack(on)
+            host = np.empty(n, np.int64) if kind == "pageable" else pinned
+            host[:] = 0x5A5A5A5A5A5A5A5A
+            st = bfs.run_bfs(root, host)
+            assert sha(g500.levels_from_pred(host)) == pr["levels_sha256"], (scale, vr, root, on, kind)
+            ok, evc, rep = oracle_mod.validate(edges, nglob, n, root, host)
+            assert ok and evc == pr["edge_visit_count"] == st.nedge, (rep, on, kind)
+    bfs.set_host_pack(True)
+    g500.check(g500.lib().g500_host_free(hp))
+    bfs.close()
+
+
 def _edges_from_pairs(g500, pairs):
     a = np.zeros(len(pairs), g500.EDGE_DTYPE)
     for i, (u, v) in enumerate(pairs):
