@@ -642,14 +642,12 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
 
   // roots: lane i starts at reorder[root_i] (a root outside the CSR range has
   // no edges; its level 0 is written by the output pass)
-  unsigned long long mf0 = 0;
   if (tid < nroots) {
     const uint32_t r = __ldg(p.reorder + p.roots[tid]);
     if ((int64_t)r < p.nlv) {
       atomicOr(p.V + (int64_t)r * NW + tid / 32, 1u << (tid & 31));
       atomicOr(p.F[0] + (int64_t)r * NW + tid / 32, 1u << (tid & 31));
       p.L[(int64_t)r * W + tid] = 0;
-      mf0 = __ldg(p.off + r + 1) - __ldg(p.off + r);
     }
   }
   if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
@@ -658,7 +656,6 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
   bool pull = false;  // the first frontier is a handful of roots
   unsigned phase = 0, pulls = 0;
   int level = 1;
-  (void)mf0;
   for (;; ++level) {
     unsigned long long* cnt = ctl->cnt[phase % 3];
     unsigned* alive = ctl->alive[phase % 3];
