@@ -61,6 +61,11 @@ constexpr int BFS_MIN_BLOCKS = 2;        // co-resident blocks per SM (64 regist
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
 constexpr int BU_WORDS = 8;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
 constexpr int BU_SERIAL = 8;              // row entries a lane checks alone (one sector) before the warp helps
+// A frontier row of more than BIG_CHUNKS work items is listed whole (up to
+// BIG_ROWS rows per level) instead of cut into items by one warp; the next
+// top-down level spreads its chunks over every warp.
+constexpr uint32_t BIG_CHUNKS = 64;
+constexpr int BIG_ROWS = 1024;
 
 struct RunParams {
   const uint64_t* __restrict__ off;
@@ -72,6 +77,7 @@ struct RunParams {
   int64_t* __restrict__ pred;
   int64_t* __restrict__ pred_r;  // deferred mode: pred entries by reordered id, [nlv]
   uint32_t* pred_p;              // the same buffer holding packed entries (deferred == 2)
+  TdItem* big;                   // [BIG_ROWS] long rows for the next top-down level (begin, deg, orig)
   int deferred;                  // 0: pred as found; 1: pred_r during the search, pred in one pass
                                  // at the end; 2: the same with packed entries
   uint32_t first_id;             // mask of the vertex id in first[] (FIRST_ID, or all bits without flags)
@@ -116,11 +122,25 @@ __device__ __forceinline__ void flush_counter(unsigned long long* c, unsigned lo
 
 // Append the chunks of one row per lane (rows of degree < 2 and lanes with no
 // row pass deg 0).  The whole warp writes the items, so a hub's thousands of
-// chunks are not left to one lane.
+// chunks are not left to one lane; a row of more than BIG_CHUNKS chunks is
+// listed whole instead (while the list has room), for the next top-down
+// level to spread over every warp.
 __device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t orig, TdItem* __restrict__ q_out,
-                                           int64_t cap, unsigned long long* qcount, BfsCtl* ctl) {
+                                           int64_t cap, unsigned long long* qcount, BfsCtl* ctl, TdItem* big,
+                                           unsigned long long* bigcount) {
   const int lane = threadIdx.x & 31;
-  const uint32_t nch = chunks_of(deg);
+  uint32_t nch = chunks_of(deg);
+  if (nch > BIG_CHUNKS && deg < (1ull << 31)) {
+    const unsigned long long bi = atomicAdd(bigcount, 1ull);
+    if (bi < (unsigned long long)BIG_ROWS) {
+      TdItem it;
+      it.begin = rb;
+      it.orig = orig;
+      it.len = (uint32_t)deg;  // < 2^31: a row is shorter than the graph's 2^31 entries per vertex
+      big[bi] = it;
+      nch = 0;
+    }
+  }
   const uint32_t incl = warp_incl_scan(nch);
   const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
   if (total == 0) return;
@@ -154,30 +174,67 @@ __device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t o
 
 // Top-down level: expand the work items, claim unvisited targets, and list the
 // discovered (vertex, original id) pairs.  Rows are cut into work items only
-// if the next level is top-down as well (chunk_phase).
+// if the next level is top-down as well (chunk_phase).  The nbig rows listed
+// whole (p.big) are expanded as virtual items qn, qn + 1, ... after the
+// queue's: item qn + c is chunk c of their concatenated chunks, found from
+// a prefix of their chunk counts that each block keeps in shared memory.
 template <int DEF>
-__device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, int64_t qn, uint32_t* vis,
+__device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, int64_t qn, int64_t nbig, uint32_t* vis,
                          uint2* __restrict__ found_list, unsigned long long* cnt, unsigned long long* sh_acc,
                          int64_t lvl) {
+  __shared__ uint32_t sh_bigpre[BIG_ROWS + 1];  // sh_bigpre[i] = chunks of big rows 0 .. i-1
   const int lane = threadIdx.x & 31;
+  int64_t nall = qn;
+  if (nbig > 0) {
+    if (threadIdx.x < 32) {
+      uint32_t run = 0;
+      if (lane == 0) sh_bigpre[0] = 0;
+      for (int64_t i0 = 0; i0 < nbig; i0 += 32) {
+        const int64_t i = i0 + lane;
+        const uint32_t c = i < nbig ? chunks_of(__ldcg(&p.big[i].len)) : 0u;
+        const uint32_t incl = warp_incl_scan(c);
+        if (i < nbig) sh_bigpre[i + 1] = run + incl;
+        run += __shfl_sync(FULL_MASK, incl, 31);
+      }
+    }
+    __syncthreads();
+    nall = qn + (int64_t)sh_bigpre[nbig];
+  }
   const int64_t nwarps = gwarp_count();
-  const int64_t per_warp = (qn + nwarps - 1) / nwarps;
+  const int64_t per_warp = (nall + nwarps - 1) / nwarps;
   const int B = per_warp >= 32 ? 32 : (per_warp < 1 ? 1 : (int)per_warp);  // items per batch
   unsigned long long found = 0, frontier = 0, edges = 0, sectors = 0, mf = 0;
-  for (int64_t base = gwarp_id() * B; base < qn; base += nwarps * B) {
+  for (int64_t base = gwarp_id() * B; base < nall; base += nwarps * B) {
     const int64_t qi = base + lane;
     uint64_t b = 0;
-    uint32_t len = 0, orig_u = 0;
+    uint32_t len = 0, orig_u = 0, first = 0;
     if (lane < B && qi < qn) {
       const TdItem it = q_in[qi];
       b = it.begin;
       len = it.len & ~FIRST_CHUNK;
       orig_u = it.orig;
-      if (p.count_edges) {
-        frontier += (it.len >> 31);
-        edges += len;
-        sectors += (len + 7) / 8;
+      first = it.len >> 31;
+    } else if (lane < B && qi < nall) {  // chunk c of the big rows: binary search of the prefix
+      const uint32_t c = (uint32_t)(qi - qn);
+      int lo = 0, hi = (int)nbig - 1;  // the row i with sh_bigpre[i] <= c < sh_bigpre[i + 1]
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sh_bigpre[mid] <= c) lo = mid;
+        else hi = mid - 1;
       }
+      const uint64_t rbeg = __ldcg(&p.big[lo].begin);
+      const uint32_t rdeg = __ldcg(&p.big[lo].len);
+      const uint32_t j = c - sh_bigpre[lo];
+      const uint64_t left = (uint64_t)rdeg - (uint64_t)j * TD_CHUNK;
+      b = rbeg + (uint64_t)j * TD_CHUNK;
+      len = (uint32_t)(left < (uint64_t)TD_CHUNK ? left : (uint64_t)TD_CHUNK);
+      orig_u = __ldcg(&p.big[lo].orig);
+      first = j == 0;
+    }
+    if (p.count_edges && len) {
+      frontier += first;
+      edges += len;
+      sectors += (len + 7) / 8;
     }
     const uint32_t incl = warp_incl_scan(len);
     const uint32_t excl = incl - len;
@@ -254,7 +311,7 @@ __device__ void chunk_phase(const RunParams& p, const uint2* __restrict__ found_
       skipped += (deg < 2);
       if (deg < 2) deg = 0;  // a degree-1 vertex only leads back to its parent
     }
-    append_row(rb, deg, ow, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
+    append_row(rb, deg, ow, q_out, p.cap, &cnt[C_QITEMS], p.ctl, p.big, &cnt[C_BIG]);
   }
   block_add(sh_acc, C_SKIP, skipped);
 }
@@ -442,7 +499,7 @@ __device__ void compact_phase(const RunParams& p, const uint32_t* __restrict__ v
         skipped += (deg < 2);
         if (deg < 2) deg = 0;
       }
-      append_row(rb, deg, ow, q_out, p.cap, &cnt[C_QITEMS], p.ctl);
+      append_row(rb, deg, ow, q_out, p.cap, &cnt[C_QITEMS], p.ctl, p.big, &cnt[C_BIG]);
     }
   }
   block_add(sh_acc, C_SKIP, skipped);
@@ -518,7 +575,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
 
   int cur_vis = 0;
   bool forward = true, growing = true;
-  int64_t qn = root_items, prev_nq = 0, visited = 1, carried = 0;
+  int64_t qn = root_items, prev_nq = 0, visited = 1, carried = 0, nbig = 0;
   int64_t mu = (int64_t)(p.off[p.nlv] - root_deg);  // degree sum of unvisited vertices (edge policy)
   unsigned phase = 0;
   int level = 1;
@@ -537,7 +594,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
     const int64_t lvl = (int64_t)level << 48;
     unsigned long long disc, scan = 0, edges, sect, front = 0, listed = 0, t_mid = 0, mf = 0;
     if (forward) {
-      td_phase<DEF>(p, items, qn, p.vis[cur_vis], found_list, cnt, sh_acc, lvl);
+      td_phase<DEF>(p, items, qn, nbig, p.vis[cur_vis], found_list, cnt, sh_acc, lvl);
       if (!grid_sync<C_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
       if (tid == 0) t_mid = globaltimer();
       ++phase;
@@ -594,6 +651,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       if (!grid_sync<C_NUM>(&ctl->bar, ccnt, sh_acc, ccnt, sh_cnt, &sh_flag)) return;
       ++phase;
       qn = (int64_t)sh_cnt[C_QITEMS];
+      nbig = (int64_t)(sh_cnt[C_BIG] < (unsigned long long)BIG_ROWS ? sh_cnt[C_BIG] : (unsigned long long)BIG_ROWS);
       carried = (int64_t)sh_cnt[C_SKIP];
       if (qn > p.cap) {  // append_row already flagged it; never read past the queue
         if (tid == 0) atomicOr(&ctl->bar.err, (unsigned)BFS_ERR_QUEUE);
@@ -700,6 +758,7 @@ static int bfs_free(g500_bfs* b) {
   dev_free(b->d_queue[1]);
   dev_free(b->d_ctl);
   dev_free(b->d_rec);
+  dev_free(b->d_big);
   if (b->h_ctl) cudaFreeHost(b->h_ctl);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
@@ -744,6 +803,7 @@ static int make_params(g500_bfs* b, int64_t root, int64_t* pred, RunParams* out)
   if (p.deferred && !b->d_pred_r) G500_TRY(dev_alloc_n(&b->d_pred_r, std::max<int64_t>(g->nlv, 1), "deferred pred"));
   p.pred_r = b->d_pred_r;
   p.pred_p = reinterpret_cast<uint32_t*>(b->d_pred_r);
+  p.big = b->d_big;
   p.vis[0] = b->d_vis[0];
   p.vis[1] = b->d_vis[1];
   p.queue[0] = b->d_queue[0];
@@ -798,6 +858,7 @@ extern "C" int g500_bfs_create(g500_graph* g, g500_bfs** out) {
   if (st == G500_OK) st = dev_alloc_n(&b->d_queue[1], b->queue_cap, "top-down discovered list");
   if (st == G500_OK) st = dev_alloc_n(&b->d_ctl, 1, "bfs control block");
   if (st == G500_OK) st = dev_alloc_n(&b->d_rec, MAX_LEVELS, "level records");
+  if (st == G500_OK) st = dev_alloc_n(&b->d_big, BIG_ROWS, "long frontier rows");
   if (st == G500_OK) chk(cudaHostAlloc(&b->h_ctl, sizeof(BfsCtl), cudaHostAllocDefault), "cudaHostAlloc");
   if (st == G500_OK) chk(cudaMemset(b->d_ctl, 0, sizeof(BfsCtl)), "cudaMemset");
   if (st == G500_OK) memset(b->h_ctl, 0, sizeof(BfsCtl));

@@ -118,7 +118,8 @@ struct g500_graph {
 };
 
 // Per-phase counters of the persistent BFS kernel (3 rotating slots).
-enum BfsCounter { C_QITEMS = 0, C_DISC, C_SCAN, C_EDGES, C_SECT, C_FRONT, C_SKIP, C_MF, C_NUM };  // C_MF: degree sum of new top-down discoveries
+// C_MF: degree sum of new top-down discoveries; C_BIG: rows listed whole for the next top-down level
+enum BfsCounter { C_QITEMS = 0, C_DISC, C_SCAN, C_EDGES, C_SECT, C_FRONT, C_SKIP, C_MF, C_BIG, C_NUM };
 
 // Top-down work item: one chunk (<= TD_CHUNK edges) of a frontier row.
 struct __align__(16) TdItem {
@@ -199,6 +200,7 @@ struct g500_bfs {
   BfsCtl* d_ctl = nullptr;
   BfsCtl* h_ctl = nullptr;           // pinned copy after each run
   LevelRecord* d_rec = nullptr;      // [MAX_LEVELS]
+  TdItem* d_big = nullptr;           // [BIG_ROWS] long frontier rows, listed whole
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int64_t last_root = -1;
 };

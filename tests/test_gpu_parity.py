@@ -231,7 +231,8 @@ def _edges_from_pairs(g500, pairs):
 
 
 @pytest.mark.parametrize("pred_mode", [1, 2, 3])  # 3 on the path graph: deeper than the packed field
-@pytest.mark.parametrize("name", ["path", "star", "two_components", "self_loops_dups", "high_ids", "isolated_root"])
+@pytest.mark.parametrize("name", ["path", "star", "big_star", "two_components", "self_loops_dups", "high_ids",
+                                  "isolated_root"])
 @pytest.mark.parametrize("vr", [0, 1, 2])
 def test_small_graphs(g500, oracle_mod, name, vr, pred_mode):
     rng = np.random.default_rng(7)
@@ -241,6 +242,9 @@ def test_small_graphs(g500, oracle_mod, name, vr, pred_mode):
         root = 0
     elif name == "star":
         pairs = [(0, i) for i in range(1, 5000)]
+        root = 17
+    elif name == "big_star":  # a hub row of 30000 edges reached top-down: listed whole, spread over the warps
+        pairs = [(0, i) for i in range(1, 30000)] + [(i, i + 30000) for i in range(1, 30000, 7)]
         root = 17
     elif name == "two_components":
         pairs = [(int(a), int(b)) for a, b in rng.integers(0, 500, (3000, 2))]
