@@ -83,20 +83,19 @@ __device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v
   return old;
 }
 
-__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 
 // Grid-wide barrier for a cooperative launch.  The block's accumulated
 // counters are first added to flush_slot (one global atomic per non-zero
 // counter per block).  Thread 0 then arrives on a counter with acquire-release
 // semantics (the block's writes, ordered before it by __syncthreads, are
-// released with it); the last arrival resets the counter and publishes the
-// next generation with a release store; the others poll the generation and
-// take an acquire fence once it moved.  Polls are bounded; on timeout (or an error raised
-// elsewhere, checked every 16 polls) the barrier reports failure and the
-// caller returns.  On success thread 0 copies read_slot into sh_cnt for the
-// block's next decision.
+// released with it).  The counter only grows during a launch (it starts at
+// zero): barrier k is complete once it reaches (k + 1) * gridDim.x, a target
+// each block computes from the value its own arrival returned, so the last
+// arrival has nothing more to publish.  The others poll the counter and take
+// an acquire fence once it reached the target.  Polls are bounded; on
+// timeout (or an error raised elsewhere, checked every 16 polls) the barrier
+// reports failure and the caller returns.  On success thread 0 copies
+// read_slot into sh_cnt for the block's next decision.
 template <int NC>
 __device__ bool grid_sync(GridBarrier* bar, unsigned long long* flush_slot, unsigned long long* sh_acc,
                           const unsigned long long* read_slot, unsigned long long* sh_cnt, unsigned* sh_flag,
@@ -110,17 +109,15 @@ __device__ bool grid_sync(GridBarrier* bar, unsigned long long* flush_slot, unsi
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* err = &bar->err;
-    volatile unsigned* gen = &bar->gen;
-    const unsigned g = *gen;
+    volatile unsigned* count = &bar->count;
     bool ok = true;
-    if (atom_add_acq_rel_gpu(&bar->count, 1u) == gridDim.x - 1) {
-      atomicExch(&bar->count, 0u);
-      st_release_gpu(&bar->gen, g + 1);
-    } else {
+    const unsigned old = atom_add_acq_rel_gpu(&bar->count, 1u);
+    const unsigned target = (old / gridDim.x + 1u) * gridDim.x;
+    if (old + 1u != target) {
       // relaxed polls (an acquire per poll would invalidate L1 under the
-      // other blocks of the SM), one acquire fence once the generation moved
+      // other blocks of the SM), one acquire fence once the target is reached
       unsigned long long spins = 0;
-      while (*gen == g) {
+      while ((int)(*count - target) < 0) {
         ++spins;
         if ((spins & 15) == 0 && *err) {
           ok = false;

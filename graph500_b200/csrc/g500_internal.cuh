@@ -131,10 +131,11 @@ enum BfsErr { BFS_ERR_QUEUE = 1, BFS_ERR_TIMEOUT = 2, BFS_ERR_DEPTH = 4, BFS_ERR
 constexpr unsigned GRID_ERR_TIMEOUT = 2;  // same bit as BFS_ERR_TIMEOUT
 
 // State of a grid-wide barrier of a cooperative kernel (device memory, zeroed
-// before each launch): arrivals, generation, sticky error bits.
+// before each launch): arrivals of every barrier of the launch so far, sticky
+// error bits.
 struct GridBarrier {
   unsigned count;
-  unsigned gen;
+  unsigned reserved;
   unsigned err;
   unsigned pad;
 };
