@@ -59,7 +59,7 @@ constexpr int PACK_SHIFT = 27;
 constexpr int PACK_LEVELS = 1 << (32 - PACK_SHIFT);
 constexpr int BFS_MIN_BLOCKS = 2;        // co-resident blocks per SM (64 registers, no spills)
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
-constexpr int BU_WORDS = 8;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
+constexpr int BU_WORDS = 4;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
 constexpr int BU_SERIAL = 8;              // row entries a lane checks alone (one sector) before the warp helps
 // A frontier row of more than BIG_CHUNKS work items is listed whole (up to
 // BIG_ROWS rows per level) instead of cut into items by one warp; the next
