@@ -59,6 +59,8 @@ def test_invalid_arguments_return_status(g500):
     assert L.g500_gen_edges(0, 16, 2, 3, 0, 10, None, 1, None) == g500.G500_E_INVAL
     assert L.g500_gen_edges(10, 16, 2, 3, 0, (1 << 10) * 16 + 1, None, 1, None) == g500.G500_E_RANGE
     assert L.g500_bfs_run(None, 0, None, 0, None) == g500.G500_E_INVAL
+    for setter in (L.g500_bfs_set_pred_mode, L.g500_bfs_set_host_pack, L.g500_bfs_set_grid):
+        assert setter(None, 0) == g500.G500_E_INVAL
 
 
 @pytest.mark.skipif(HAS_GPU, reason="checks the no-device error path")
