@@ -101,8 +101,9 @@ __device__ __forceinline__ void store_mask(uint32_t* p, const Mask<NW>& m) {
 // Frontier masks gathered by the pull phase use plain loads, which may hit
 // L1: hub rows recur in many adjacency lists.  The masks are rewritten by the
 // apply pass of the same launch; the grid barrier between that pass and the
-// next level (fence and atomic arrive on one side, fence after the generation
-// is seen on the other) orders those writes before these loads.
+// next level (an acquire-release arrival on one side, an acquire fence once
+// the arrival count is seen complete on the other) orders those writes before
+// these loads.
 template <int NW>
 __device__ __forceinline__ Mask<NW> gather_mask(const uint32_t* p) {
   Mask<NW> m;
