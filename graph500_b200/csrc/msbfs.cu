@@ -44,6 +44,7 @@ struct MsCtl {
   unsigned long long t0_ns, t_init_ns, t_end_ns;
   unsigned alive[3][4];      // lanes that found vertices in the phase (rotating like cnt)
   unsigned long long level_new[MS_MAX_LEVEL + 2];
+  unsigned long long lane_deg[MS_MAX_LANES];  // sampled frontier degree sum per lane (lane survey)
   unsigned long long level_t_ns[MS_MAX_LEVEL + 2];
   unsigned long long level_mid_ns[MS_MAX_LEVEL + 2];  // end of the pull/push phase
   unsigned char level_pull[MS_MAX_LEVEL + 2];
@@ -227,7 +228,10 @@ __device__ __forceinline__ void settle(const MsParams& p, uint32_t* Fn, int64_t 
 // Each row is its own only writer, so it settles at once (next frontier,
 // visited mask, levels): pull levels need no separate apply pass over all
 // vertices, only one over the hub rows.
-template <int NW>
+// INTO_N (a level that pulls some lanes and pushes the others): a row's
+// finds go into its next mask N, beside the push's, for the apply pass to
+// settle, instead of settling here.
+template <int NW, bool INTO_N>
 __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, const uint32_t* Fc, uint32_t* Fn,
                              uint32_t lvl4, LevelAcc<NW>& la) {
   const int lane = threadIdx.x & 31;
@@ -311,7 +315,13 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, const uint3
       Mask<NW> nw;
 #pragma unroll
       for (int k = 0; k < NW; ++k) nw.w[k] = acc.w[k] & need.w[k];
-      settle<NW>(p, Fn, v, vv, need, nw, deg, lvl4, la);
+      if constexpr (INTO_N) {
+#pragma unroll
+        for (int k = 0; k < NW; ++k)
+          if (nw.w[k]) atomicOr(p.N + v * NW + k, nw.w[k]);
+      } else {
+        settle<NW>(p, Fn, v, vv, need, nw, deg, lvl4, la);
+      }
     }
   }
 }
@@ -402,7 +412,7 @@ __device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act, const uint3
 // push from hub frontier rows: every neighbour of the chunk gets the lanes it
 // still lacks
 template <int NW>
-__device__ void ms_push_hubs(const MsParams& p, const uint32_t* Fc) {
+__device__ void ms_push_hubs(const MsParams& p, const uint32_t* Fc, const Mask<NW>& qm) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = gwarp_count();
   for (int64_t c0 = gwarp_id(); c0 < p.npush_chunks; c0 += 32 * nwarps) {
@@ -416,7 +426,10 @@ __device__ void ms_push_hubs(const MsParams& p, const uint32_t* Fc) {
       hd = __ldg(p.push_tab + c);
       f = load_mask<NW>(Fc + (int64_t)hd.x * NW);
 #pragma unroll
-      for (int k = 0; k < NW; ++k) any |= f.w[k] != 0;
+      for (int k = 0; k < NW; ++k) {
+        f.w[k] &= qm.w[k];
+        any |= f.w[k] != 0;
+      }
     }
     unsigned todo = __ballot_sync(FULL_MASK, any);
     while (todo) {
@@ -456,17 +469,21 @@ __device__ void ms_push_hubs(const MsParams& p, const uint32_t* Fc) {
 // edges walked as one list, MS_WIN at a time; every neighbour gets the lanes
 // it still lacks.
 template <int NW>
-__device__ void ms_push_rows(const MsParams& p, const uint32_t* Fc) {
+__device__ void ms_push_rows(const MsParams& p, const uint32_t* Fc, const Mask<NW>& qm) {
   const int lane = threadIdx.x & 31;
   for (int64_t base = gwarp_id() * (32 * MS_GROUPS); base < p.nlv; base += gwarp_count() * (32 * MS_GROUPS)) {
     Mask<NW> fg[MS_GROUPS];
 #pragma unroll
     for (int g = 0; g < MS_GROUPS; ++g) {
       const int64_t v = base + g * 32 + lane;
-      if (v < p.nlv) fg[g] = load_mask<NW>(Fc + v * NW);
-      else
+      if (v < p.nlv) {
+        fg[g] = load_mask<NW>(Fc + v * NW);
+#pragma unroll
+        for (int k = 0; k < NW; ++k) fg[g].w[k] &= qm.w[k];
+      } else {
 #pragma unroll
         for (int k = 0; k < NW; ++k) fg[g].w[k] = 0;
+      }
     }
 #pragma unroll
     for (int g = 0; g < MS_GROUPS; ++g) {
@@ -588,6 +605,47 @@ __device__ void ms_settle_hubs(const MsParams& p, const Mask<NW>& act, uint32_t*
   }
 }
 
+// Lane survey before a level that would pull: the frontier degree sum of each
+// lane, estimated from every MS_SURVEY_STEP-th vertex.  A lane with a small
+// frontier finds few vertices at this level, yet while any of its vertices
+// stay unfound every row that still needs it is scanned to its end; such
+// lanes are pushed instead.  Per 32 sampled vertices a warp reduces each
+// lane bit's degrees (lane b of the warp keeps bits b, b + 32, ...), then
+// the block adds them up in shared memory and once into ctl->lane_deg.
+constexpr int MS_SURVEY_STEP = 8;
+template <int NW>
+__device__ void ms_lane_survey(const MsParams& p, const uint32_t* Fc, unsigned long long* sh_lane) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long acc[NW];
+#pragma unroll
+  for (int k = 0; k < NW; ++k) acc[k] = 0;
+  const int64_t nsample = (p.nlv + MS_SURVEY_STEP - 1) / MS_SURVEY_STEP;
+  for (int64_t base = gwarp_id() * 32; base < nsample; base += gwarp_count() * 32) {
+    const int64_t v = (base + lane) * MS_SURVEY_STEP;
+    Mask<NW> f;
+    uint32_t d = 0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) f.w[k] = 0;
+    if (v < p.nlv) {
+      f = load_mask<NW>(Fc + v * NW);
+      d = __ldg(p.deg + v);
+    }
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) any |= f.w[k] != 0;
+    if (!__any_sync(FULL_MASK, any)) continue;
+#pragma unroll
+    for (int k = 0; k < NW; ++k)
+      for (int b = 0; b < 32; ++b) {
+        const unsigned sum = __reduce_add_sync(FULL_MASK, ((f.w[k] >> b) & 1u) ? d : 0u);
+        if (lane == b) acc[k] += sum;
+      }
+  }
+#pragma unroll
+  for (int k = 0; k < NW; ++k)
+    if (acc[k]) atomicAdd(&sh_lane[k * 32 + lane], acc[k]);
+}
+
 // the level's counters into the block accumulators, and the lanes that found
 // vertices (the others have finished their BFS) into alive_out
 template <int NW>
@@ -655,8 +713,12 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
 
   if (tid == 0) ctl->t_init_ns = globaltimer();
   bool pull = false;  // the first frontier is a handful of roots
+  bool surveyed = false;
   unsigned phase = 0, pulls = 0;
   int level = 1;
+  __shared__ unsigned long long sh_lane[MS_MAX_LANES];
+  __shared__ uint32_t sh_qm[4];
+  const unsigned long long survey_thr = __ldg(p.off + p.nlv) / (64ull * MS_SURVEY_STEP);
   for (;; ++level) {
     unsigned long long* cnt = ctl->cnt[phase % 3];
     unsigned* alive = ctl->alive[phase % 3];
@@ -667,17 +729,63 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
     const uint32_t lvl4 = (uint32_t)level * 0x01010101u;
     LevelAcc<NW> la;
     la.clear();
+    // The first level that would pull surveys the lanes' frontiers: lanes
+    // whose frontier degree sum is under 1/64 of the graph's entries are
+    // pushed at that level, the others pulled (a mixed level: both phases
+    // leave their finds in N and the apply pass settles every vertex).
+    Mask<NW> qm, pm;  // lanes pushed, lanes pulled
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      qm.w[k] = pull ? 0u : ~0u;
+      pm.w[k] = act.w[k];
+    }
+    if (pull && !surveyed) {
+      surveyed = true;
+      for (int i = threadIdx.x; i < MS_MAX_LANES; i += blockDim.x) sh_lane[i] = 0;
+      __syncthreads();
+      ms_lane_survey<NW>(p, Fc, sh_lane);
+      __syncthreads();
+      if (threadIdx.x < W && sh_lane[threadIdx.x]) atomicAdd(&ctl->lane_deg[threadIdx.x], sh_lane[threadIdx.x]);
+      if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
+      if (threadIdx.x < NW) {
+        uint32_t q = 0;
+        for (int b = 0; b < 32; ++b) {
+          const int k = threadIdx.x * 32 + b;
+          if (((act.w[threadIdx.x] >> b) & 1u) && __ldcg(&ctl->lane_deg[k]) < survey_thr) q |= 1u << b;
+        }
+        sh_qm[threadIdx.x] = q;
+      }
+      __syncthreads();
+      bool anyp = false;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        qm.w[k] = sh_qm[k];
+        pm.w[k] = act.w[k] & ~qm.w[k];
+        anyp |= pm.w[k] != 0;
+      }
+      if (!anyp) pull = false;  // every live lane is small: a push level
+    }
+    bool mixed = false;
     if (pull) {
-      ms_pull_rows<NW>(p, act, Fc, Fn, lvl4, la);
+#pragma unroll
+      for (int k = 0; k < NW; ++k) mixed |= qm.w[k] != 0;
+    }
+    if (pull && !mixed) {
+      ms_pull_rows<NW, false>(p, act, Fc, Fn, lvl4, la);
       ms_pull_hubs<NW>(p, act, Fc);
+    } else if (mixed) {
+      ms_push_rows<NW>(p, Fc, qm);
+      ms_push_hubs<NW>(p, Fc, qm);
+      ms_pull_rows<NW, true>(p, pm, Fc, Fn, lvl4, la);
+      ms_pull_hubs<NW>(p, pm, Fc);
     } else {
-      ms_push_rows<NW>(p, Fc);
-      ms_push_hubs<NW>(p, Fc);
+      ms_push_rows<NW>(p, Fc, qm);
+      ms_push_hubs<NW>(p, Fc, qm);
     }
     pulls += pull;
     if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
     if (tid == 0) ctl->level_mid_ns[level] = globaltimer();
-    if (pull) ms_settle_hubs<NW>(p, act, Fn, lvl4, la);
+    if (pull && !mixed) ms_settle_hubs<NW>(p, act, Fn, lvl4, la);
     else ms_apply<NW>(p, act, Fn, lvl4, la);
     flush_level<NW>(la, sh_acc, sh_or, alive);
     if (!grid_sync<M_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
@@ -686,7 +794,7 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
     if (tid == 0) {
       ctl->level_new[level] = nnew;
       ctl->level_t_ns[level] = globaltimer();
-      ctl->level_pull[level] = pull ? 1 : 0;
+      ctl->level_pull[level] = pull ? (mixed ? 2 : 1) : 0;
     }
     // a lane that found nothing this level has finished: it no longer needs anything
     {

@@ -277,7 +277,8 @@ int g500_msbfs_device_levels(const g500_msbfs* m, const uint8_t** dev_levels);
  * pairs it discovered, and its device time from the kernel's global timer. */
 typedef struct g500_msbfs_level {
   int32_t level;
-  int32_t pull;            /* 1 = pull (unvisited lanes look at the frontier), 0 = push */
+  int32_t pull;            /* 1 = pull (unvisited lanes look at the frontier), 0 = push, 2 = both: the
+                              lanes with a small frontier pushed, the others pulled */
   int64_t discovered;      /* new (vertex, lane) pairs */
   double device_ms;        /* the whole level */
   double expand_ms;        /* its pull or push phase (the rest is the apply pass) */
