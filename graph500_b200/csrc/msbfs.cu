@@ -613,6 +613,7 @@ __device__ void ms_settle_hubs(const MsParams& p, const Mask<NW>& act, uint32_t*
 // lane bit's degrees (lane b of the warp keeps bits b, b + 32, ...), then
 // the block adds them up in shared memory and once into ctl->lane_deg.
 constexpr int MS_SURVEY_STEP = 8;
+constexpr int MS_SURVEY_DIV = 64;  // a lane is pushed when its frontier degree sum is under entries / this
 template <int NW>
 __device__ void ms_lane_survey(const MsParams& p, const uint32_t* Fc, unsigned long long* sh_lane) {
   const int lane = threadIdx.x & 31;
@@ -718,7 +719,7 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
   int level = 1;
   __shared__ unsigned long long sh_lane[MS_MAX_LANES];
   __shared__ uint32_t sh_qm[4];
-  const unsigned long long survey_thr = __ldg(p.off + p.nlv) / (64ull * MS_SURVEY_STEP);
+  const unsigned long long survey_thr = __ldg(p.off + p.nlv) / ((unsigned long long)MS_SURVEY_DIV * MS_SURVEY_STEP);
   for (;; ++level) {
     unsigned long long* cnt = ctl->cnt[phase % 3];
     unsigned* alive = ctl->alive[phase % 3];
@@ -730,7 +731,7 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
     LevelAcc<NW> la;
     la.clear();
     // The first level that would pull surveys the lanes' frontiers: lanes
-    // whose frontier degree sum is under 1/64 of the graph's entries are
+    // whose frontier degree sum is under 1/MS_SURVEY_DIV of the graph's entries are
     // pushed at that level, the others pulled (a mixed level: both phases
     // leave their finds in N and the apply pass settles every vertex).
     Mask<NW> qm, pm;  // lanes pushed, lanes pulled
