@@ -614,6 +614,7 @@ __device__ void ms_settle_hubs(const MsParams& p, const Mask<NW>& act, uint32_t*
 // the block adds them up in shared memory and once into ctl->lane_deg.
 constexpr int MS_SURVEY_STEP = 8;
 constexpr int MS_SURVEY_DIV = 64;  // a lane is pushed when its frontier degree sum is under entries / this
+constexpr int MS_SURVEY_LEVELS = 1;  // pull levels that survey (the first ones)
 template <int NW>
 __device__ void ms_lane_survey(const MsParams& p, const uint32_t* Fc, unsigned long long* sh_lane) {
   const int lane = threadIdx.x & 31;
@@ -714,7 +715,7 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
 
   if (tid == 0) ctl->t_init_ns = globaltimer();
   bool pull = false;  // the first frontier is a handful of roots
-  bool surveyed = false;
+  int surveys = 0;
   unsigned phase = 0, pulls = 0;
   int level = 1;
   __shared__ unsigned long long sh_lane[MS_MAX_LANES];
@@ -740,8 +741,9 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
       qm.w[k] = pull ? 0u : ~0u;
       pm.w[k] = act.w[k];
     }
-    if (pull && !surveyed) {
-      surveyed = true;
+    const bool survey = pull && surveys < MS_SURVEY_LEVELS;
+    if (survey) {
+      ++surveys;
       for (int i = threadIdx.x; i < MS_MAX_LANES; i += blockDim.x) sh_lane[i] = 0;
       __syncthreads();
       ms_lane_survey<NW>(p, Fc, sh_lane);
@@ -786,6 +788,10 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
     pulls += pull;
     if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
     if (tid == 0) ctl->level_mid_ns[level] = globaltimer();
+    // every block read the survey's sums before this barrier; the next
+    // survey adds after the level's closing one
+    if (survey && blockIdx.x == 0)
+      for (int i = threadIdx.x; i < MS_MAX_LANES; i += blockDim.x) ctl->lane_deg[i] = 0;
     if (pull && !mixed) ms_settle_hubs<NW>(p, act, Fn, lvl4, la);
     else ms_apply<NW>(p, act, Fn, lvl4, la);
     flush_level<NW>(la, sh_acc, sh_or, alive);
