@@ -63,3 +63,13 @@ def g500():
     import graph500_b200
     graph500_b200.lib()
     return graph500_b200
+
+
+# the benchmark sizes, pinned by per-root records of the unmodified reference
+# (tests/golden/make_golden.py --large)
+LARGE_GOLDEN_CASES = [(22, 2), (24, 2)]
+
+
+def load_golden_record(scale: int, vr: int):
+    with open(os.path.join(GOLDEN, f"ref_s{scale}_vr{vr}.json")) as f:
+        return json.load(f)

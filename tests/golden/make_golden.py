@@ -8,6 +8,10 @@ and stores, per (SCALE, VERTEX_REORDERING) case:
   - per root: edge_visit_count, a digest of the level array ((pred>>48)&0xFFFF),
     the level histogram, and for two roots the full level array,
   - one reference predecessor array (SCALE 12, VR 0, first root).
+The benchmark sizes (SCALE 22 and 24, VR 2, the 64 find_roots roots) keep the
+per-root records only: no full level arrays, and the reference validator runs
+on the first VALIDATE_LARGE roots (every root's edge_visit_count still comes
+from it for those; the rest carry the reached count from the level histogram).
 pf_nedge.json restates the reference's known-answer table pf_nedge[]
 (mpi/utils.hpp:3663-3707, edgefactor 16, seeds 2/3).
 
@@ -29,6 +33,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 CASES = [(10, 0, 16), (12, 0, 16), (12, 2, 16), (16, 0, 16), (16, 2, 16), (18, 2, 8)]
+# the benchmark sizes (Kronecker SCALE 22 and 24, edgefactor 16, VR 2, 64 roots)
+LARGE_CASES = [(22, 2, 64), (24, 2, 64)]
+VALIDATE_LARGE = 64
 
 # mpi/utils.hpp:3663-3699: expected traversed edges for edgefactor 16, seeds (2, 3)
 PF_NEDGE = [-1, 32, 64, 128, 256, 512, 1024, 2048, 4096, 8192, 16383, 32767, 65535, 131070, 262144, 524285,
@@ -43,6 +50,7 @@ def digest(a: np.ndarray) -> str:
 
 def one_case(scale: int, vr: int, nroots: int) -> None:
     import oracle as O
+    large = scale >= 20
     ref = O.Reference(vr)
     ref.generate(scale, 16)
     edges = ref.edges()
@@ -51,30 +59,46 @@ def one_case(scale: int, vr: int, nroots: int) -> None:
     ref.prepare_bfs()
     rec = {"scale": scale, "vr": vr, "info": ref.info, "roots": roots.tolist(), "num_edges": len(edges),
            "edges_sha256": digest(edges), "per_root": []}
+    head, tail = edges[:64].copy(), edges[-64:].copy()
+    if large:
+        del edges
     full = {}
     for i, r in enumerate(roots):
-        pred, _ = ref.run_bfs(int(r))
-        ok, evc = ref.validate(int(r), pred)
-        assert ok, (scale, vr, r)
+        pred, t = ref.run_bfs(int(r))
+        entry = {"root": int(r)}
+        if not large or i < VALIDATE_LARGE:
+            ok, evc = ref.validate(int(r), pred)
+            assert ok, (scale, vr, r)
+            entry["edge_visit_count"] = evc
         lv = ((pred >> 48) & 0xFFFF).astype(np.uint16)
         lv[pred == -1] = 0xFFFF
         hist = np.bincount(np.where(lv == 0xFFFF, 0, lv.astype(np.int64) + 1)).tolist()
-        rec["per_root"].append({"root": int(r), "edge_visit_count": evc, "levels_sha256": digest(lv),
-                                "level_hist": hist})
-        if i < 2:
+        entry.update({"levels_sha256": digest(lv), "level_hist": hist})
+        rec["per_root"].append(entry)
+        if large:
+            print(f"SCALE {scale} root {i} {int(r)} bfs {t:.3f}s", file=sys.stderr, flush=True)
+        elif i < 2:
             full[f"levels_{i}"] = lv
         if scale == 12 and vr == 0 and i == 0:
             full["pred_0"] = pred
     name = f"ref_s{scale}_vr{vr}"
     with open(os.path.join(HERE, name + ".json"), "w") as f:
         json.dump(rec, f, indent=1)
-    np.savez_compressed(os.path.join(HERE, name + ".npz"), edges_head=edges[:64], edges_tail=edges[-64:], **full)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), edges_head=head, edges_tail=tail, **full)
     print("wrote", name, file=sys.stderr)
 
 
 def main() -> None:
+    """No arguments: the small cases.  ``--large``: the benchmark sizes (minutes
+    of reference construction and validation each).  ``SCALE VR NROOTS``: one case."""
     if len(sys.argv) == 4:
         one_case(int(sys.argv[1]), int(sys.argv[2]), int(sys.argv[3]))
+        return
+    if sys.argv[1:] == ["--large"]:
+        env = dict(os.environ, NO_AFFINITY="1")
+        for scale, vr, nroots in LARGE_CASES:
+            subprocess.run([sys.executable, __file__, str(scale), str(vr), str(nroots)], check=True, env=env,
+                           stdout=subprocess.DEVNULL)
         return
     with open(os.path.join(HERE, "pf_nedge.json"), "w") as f:
         json.dump({"source": "mpi/utils.hpp:3663-3707 (edgefactor 16, seeds 2/3)", "pf_nedge": PF_NEDGE}, f,
