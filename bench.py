@@ -26,6 +26,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 import numpy as np
@@ -52,8 +53,11 @@ def parse_args():
     ap.add_argument("--policy", type=int, default=0, help="direction policy with fixed alpha/beta: 0 reference, 1 edges")
     ap.add_argument("--tune-roots", type=int, default=8, help="roots the autotuner samples (untimed)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-roots", type=int, default=8, help="roots in the bounded CPU-baseline sample")
-    ap.add_argument("--ref-roots-per-step", type=int, default=4)
+    ap.add_argument("--cpu-samples", default="22:16:4,24:8:4,26:4:2",
+                    help="CPU baselines of the reference beside the GPU sections, SCALE:ROOTS:PASSES each "
+                         "(ROOTS validated find_roots roots, timed PASSES times)")
+    ap.add_argument("--ref-roots-per-step", type=int, default=None,
+                    help="reference arm: roots per step (default: --roots, the GPU arm's step)")
     ap.add_argument("--extra-scales", default="24,26",
                     help="graph sizes measured beside the main one (plain + batched), comma-separated; '' for none")
     ap.add_argument("--no-serving", action="store_true")
@@ -179,8 +183,12 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- CPU baseline
+def ref_exe(reorder: int) -> str:
+    return os.path.join(ROOT, "oracle", "_ref", f"ref_bench_vr{reorder}")
+
+
 def run_ref_bench(scale, ef, nroots, warmup, steps, per_step, reorder):
-    exe = os.path.join(ROOT, "oracle", "_ref", f"ref_bench_vr{reorder}")
+    exe = ref_exe(reorder)
     if not os.path.exists(exe):
         return None, f"{exe} not built"
     cores = os.cpu_count() or 1
@@ -205,12 +213,102 @@ def cpu_model() -> str:
     return "unknown"
 
 
+def host_ram_gb() -> float:
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) / (1 << 20)
+    except OSError:
+        pass
+    return 0.0
+
+
+class RefBaselines:
+    """The reference's own run_bfs (oracle/_ref/ref_bench_vr<N>, OpenMP on all
+    host cores) at several graph sizes, for the cpu_baseline of each section.
+
+    Generation, construction and validation take minutes at SCALE 26, so the
+    processes start with the bench, one after another at the lowest CPU
+    priority, overlapping the GPU work; each stops at its gate once its graph is
+    built and its sample roots validated.  The timed runs of each sample happen
+    one process at a time after the GPU timing, while nothing else runs."""
+
+    RAM_GB = {22: 8, 24: 24, 26: 80}  # host memory a reference process needs (generation + construction)
+
+    def __init__(self, plan, ef: int, reorder: int):
+        self.plan, self.ef, self.reorder = plan, ef, reorder  # [(scale, roots, passes)]
+        self.ready, self.err = {}, {}
+        self.cores = os.cpu_count() or 1
+        self.thread = threading.Thread(target=self._build_all, daemon=True)
+        self.thread.start()
+
+    def _build_all(self):
+        exe = ref_exe(self.reorder)
+        env = dict(os.environ, OMP_NUM_THREADS=str(self.cores))
+        env.pop("NO_AFFINITY", None)
+        for scale, roots, passes in self.plan:
+            if not os.path.exists(exe):
+                self.err[scale] = f"{exe} not built"
+                continue
+            need = self.RAM_GB.get(scale, 4 << max(0, scale - 22))
+            have = host_ram_gb()
+            if have < need:
+                self.err[scale] = f"host has {have:.0f} GB available, the reference needs about {need} GB at SCALE {scale}"
+                continue
+            log = tempfile.TemporaryFile(mode="w+")
+            p = subprocess.Popen([exe, str(scale), str(self.ef), str(roots), "0", str(passes), str(roots), "gate"],
+                                 stdin=subprocess.PIPE, stdout=subprocess.PIPE, stderr=log, text=True, env=env,
+                                 preexec_fn=lambda: os.nice(19))
+            line = p.stdout.readline()
+            if line.strip() != "ready":
+                p.wait()
+                log.seek(0)
+                tail = log.read().strip().splitlines()[-1:]
+                self.err[scale] = f"ref_bench exit {p.returncode}: {tail}"
+                continue
+            self.ready[scale] = (p, log, roots, passes)
+
+    def time_all(self) -> dict:
+        """Time every built sample in turn; {scale: cpu_baseline dict}."""
+        self.thread.join()
+        out = {}
+        for scale, roots, passes in self.plan:
+            if scale not in self.ready:
+                out[scale] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                              "sample": f"unavailable: {self.err.get(scale, 'not built')}"}
+                continue
+            p, log, roots, passes = self.ready.pop(scale)
+            stdout, _ = p.communicate("go\n")
+            log.close()
+            if p.returncode != 0:
+                out[scale] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                              "sample": f"unavailable: ref_bench exit {p.returncode}"}
+                continue
+            rec = json.loads(stdout.strip().splitlines()[-1])
+            runs = rec["runs"]
+            value = sum(x[3] for x in runs) / sum(x[2] for x in runs) / 1e9
+            out[scale] = {"value": value, "unit": UNIT, "cores": self.cores, "kind": "reference",
+                          "sample": f"{len(runs)} timed runs ({passes} passes over the first {roots} find_roots "
+                                    f"roots, each validated) of the reference run_bfs at SCALE {scale} "
+                                    f"(edgefactor {self.ef}, VERTEX_REORDERING {self.reorder}), OMP {self.cores} "
+                                    f"threads, {cpu_model()}",
+                          "construction_s": rec["construction_s"], "generation_s": rec["generation_s"]}
+        return out
+
+    def close(self):
+        for p, log, _, _ in self.ready.values():
+            p.kill()
+            p.wait()
+            log.close()
+        self.ready.clear()
+
+
 def reference_arm(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    rec, err = run_ref_bench(a.scale, a.edgefactor, min(a.roots, 64), a.warmup, a.steps, a.ref_roots_per_step,
-                             a.reorder)
+    per_step = a.ref_roots_per_step or a.roots
+    rec, err = run_ref_bench(a.scale, a.edgefactor, min(a.roots, 64), a.warmup, a.steps, per_step, a.reorder)
     if rec is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
         return
@@ -222,11 +320,11 @@ def reference_arm(a):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1000.0 * t / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic (Graph500 Kronecker generator, seeds 2/3)",
-            "impl": "reference", "config": dict(workload(a), roots_per_step=a.ref_roots_per_step,
+            "impl": "reference", "config": dict(workload(a), roots_per_step=per_step,
                                                  parallelism="1 process, OpenMP"),
             "harmonic_mean_gteps": hm / 1e9,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": rec["cores"], "kind": "reference",
-                             "sample": f"{len(runs)} BFS runs ({a.ref_roots_per_step} roots/step) of the "
+                             "sample": f"{len(runs)} BFS runs ({per_step} roots/step) of the "
                                        f"reference run_bfs at SCALE {a.scale}, {cpu_model()}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "generation_s": rec["generation_s"], "construction_s": rec["construction_s"]}
@@ -242,20 +340,18 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_bfs(a):
-    """DRAM bytes of one bfs_persistent_kernel launch from the committed ncu
-    summary for this workload (profiles/bfs_persistent_kernel_s<SCALE>.md,
-    line 'traffic_per_launch_bytes: N'), or None when there is none."""
-    p = os.path.join(ROOT, "profiles", f"bfs_persistent_kernel_s{a.scale}.md")
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.strip().startswith("traffic_per_launch_bytes:"):
-            try:
-                return float(line.split(":", 1)[1])
-            except ValueError:
-                return None
-    return None
+def traffic_per_launch(kernel: str, scale: int):
+    """DRAM bytes (read + write) of one launch of `kernel` at SCALE `scale`, as
+    one ncu capture measured them (profiles/dram_traffic.json, a data file
+    written from the capture, with the command that made it), and that
+    record's source; (None, None) without a capture of this size."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        d = json.load(open(p))
+        rec = d["kernels"][kernel][str(scale)]
+        return float(rec["bytes_per_launch"]), rec.get("source", "ncu")
+    except (OSError, KeyError, ValueError, TypeError):
+        return None, None
 
 
 def bytes_model(levels, pred_size, nlv):
@@ -272,6 +368,7 @@ def bytes_model(levels, pred_size, nlv):
 
 
 def batched_arm(a, g5, torch, bfs, roots, nedge, pred_dev, local, reduce_max, reduce_sum, barrier) -> dict:
+    peak, peak_kind = load_peaks()
     """MS-BFS over the same roots: autotune (untimed), check every root's levels
     against the plain BFS (untimed), then time K launches of all roots."""
     ms = g5.MultiSourceBFS(bfs.graph_, 64, 15.0, True)
@@ -285,6 +382,18 @@ def batched_arm(a, g5, torch, bfs, roots, nedge, pred_dev, local, reduce_max, re
         lv = torch.where(pred_dev == -1, torch.full_like(lv, 255), lv).to(torch.uint8)
         if not torch.equal(lv, out[i]):
             raise SystemExit(f"batched levels differ from the plain BFS for root {root}")
+    # bytes model of one launch (untimed counting run, same levels): per level
+    # the three mask passes, 8 B per row offset read and 32 B per adjacency
+    # sector examined; plus the uint8 level rows written
+    info = bfs.graph_.info
+    lanes = tune["lane_width"]
+    ms.set_count(True)
+    ms.run(r[:lanes])
+    counted = ms.level_info(0)
+    ms.set_count(False)
+    mask_bytes = 3 * (lanes // 8) * info.num_local_verts
+    level_bytes = [mask_bytes + 8 * l["rows_read"] + 32 * l["sectors"] for l in counted]
+    bytes_per_launch = sum(level_bytes) + min(len(r), lanes) * info.pred_size
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(a.warmup):
         ms.run(r)
@@ -300,11 +409,22 @@ def batched_arm(a, g5, torch, bfs, roots, nedge, pred_dev, local, reduce_max, re
     barrier()
     t_max = reduce_max(t / 1000.0)
     e_all = reduce_sum(float(a.steps * sum(nedge)))
+    launches = a.steps * ((len(r) + lanes - 1) // lanes)
+    ms_per_launch = t / launches
+    achieved = bytes_per_launch / (ms_per_launch / 1000.0) / 1e9
     ms.close()
     return {"metric": "aggregate GTEPS of batched multi-source BFS (same graph, same roots)",
-            "value": e_all / t_max / 1e9, "unit": UNIT, "roots_per_launch": int(min(len(r), tune["lane_width"])),
-            "roots": int(len(r)), "lane_width": tune["lane_width"], "alpha": tune["alpha"],
+            "value": e_all / t_max / 1e9, "unit": UNIT, "roots_per_launch": int(min(len(r), lanes)),
+            "roots": int(len(r)), "lane_width": lanes, "alpha": tune["alpha"],
             "ms_per_step": 1000.0 * t_max / a.steps, "levels": levels, "pull_levels": pulls,
+            "roofline": {"bound": "hbm", "kernel": "msbfs_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "bytes_per_launch": bytes_per_launch, "ms_per_launch": ms_per_launch,
+                         "bytes_model": "sum over levels of 3 mask passes (lane_width/8 B per vertex each) + "
+                                        "8 B per row offset read + 32 B per adjacency sector examined, "
+                                        "+ roots x pred_size B of uint8 levels (counted on the device)",
+                         "level_bytes": level_bytes,
+                         "level_pull": [l["pull"] for l in counted]},
             "output": "uint8 level array per root in original-id order, on the device",
             "parity": "levels of every root equal the plain BFS's (pred >> 48)"}
 
@@ -355,12 +475,14 @@ def scale_section(a, g5, torch, scale, reduce_max, reduce_sum, barrier, peak) ->
            "plain_tuning": {k: tune[k] for k in ("policy", "alpha", "beta")},
            "plain_roofline": {"bound": "hbm", "kernel": "bfs_persistent_kernel", "achieved": achieved, "peak": peak,
                               "unit": "GB/s", "frac": achieved / peak,
+                              "traffic": traffic_per_launch("bfs_persistent_kernel", scale)[0],
+                              "traffic_source": traffic_per_launch("bfs_persistent_kernel", scale)[1],
                               "bytes_per_launch": sum(model) / len(model)},
            "graph": {"num_global_verts": info.num_global_verts, "num_global_edges": info.num_global_edges,
                      "generation_s": gen_s, "construction_s": build_s}}
     bat = batched_arm(a, g5, torch, bfs, roots, nedge, pred, 0, reduce_max, reduce_sum, barrier)
     out["batched"] = {k: bat[k] for k in ("value", "unit", "lane_width", "alpha", "ms_per_step", "levels",
-                                          "pull_levels", "parity")}
+                                          "pull_levels", "roofline", "parity")}
     out["batched"]["speedup_vs_plain"] = bat["value"] / plain if plain else None
     bfs.close()
     del pred, flush
@@ -420,6 +542,17 @@ def our_arm(a):
 
     rep = Replicas(dist, "cuda")
     barrier, reduce_max, reduce_sum = rep.barrier, rep.max, rep.sum
+    # the reference's CPU samples build in the background while the GPU works (rank 0 of one process only)
+    ref_base = None
+    if world == 1 and not a.no_cpu_baseline:
+        sizes = {a.scale} | {int(x) for x in a.extra_scales.split(",") if x}
+        plan = []
+        for item in a.cpu_samples.split(","):
+            if item:
+                sc, nr, ps = (int(x) for x in item.split(":"))
+                if sc in sizes:
+                    plan.append((sc, nr, ps))
+        ref_base = RefBaselines(plan, a.edgefactor, a.reorder)
 
     bfs = g5.BfsOnGPU(device=local, reorder_mode=a.reorder)
     t0 = time.time()
@@ -497,14 +630,15 @@ def our_arm(a):
     for r in roots[:4]:
         bfs.run_bfs(int(r), host_pred)
     barrier()
-    e2e_t = 0.0
+    e2e_t = e2e_dev = 0.0
     for _ in range(a.steps):
         for r in roots:
             flush.zero_()
             torch.cuda.synchronize()
             w0 = time.perf_counter()
-            bfs.run_bfs(int(r), host_pred)
+            st = bfs.run_bfs(int(r), host_pred)
             e2e_t += time.perf_counter() - w0
+            e2e_dev += st.device_ms / 1000.0
     barrier()
     e2e_max = reduce_max(e2e_t)
     e2e_value = e_all / e2e_max / 1e9
@@ -517,6 +651,10 @@ def our_arm(a):
     sections = {}
     for sc in [int(x) for x in a.extra_scales.split(",") if x]:
         sections[f"scale{sc}"] = scale_section(a, g5, torch, sc, reduce_max, reduce_sum, barrier, peak)
+    cpu = ref_base.time_all() if ref_base else {}
+    for sc, sec in sections.items():
+        if int(sc[5:]) in cpu:
+            sec["cpu_baseline"] = cpu[int(sc[5:])]
     serving = None if a.no_serving else serving_arm(a, g5, torch, reduce_sum, barrier)
 
     if rank != 0:
@@ -540,10 +678,16 @@ def our_arm(a):
         "harmonic_mean_gteps": hm,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * len(roots),
                 "d2h_bytes_per_step": pred_bytes * info.pred_size * len(roots),
-                "path": "g500_bfs_run into a pinned host int64 pred (one DMA copy per root)"},
+                "path": "g500_bfs_run into a pinned host int64 pred (one DMA copy per root)",
+                "ms_per_root": 1000.0 * e2e_t / (a.steps * len(roots)),
+                "split_ms_per_root": {"bfs_device": 1000.0 * e2e_dev / (a.steps * len(roots)),
+                                      "pred_copy_and_host": 1000.0 * (e2e_t - e2e_dev) / (a.steps * len(roots))},
+                "pcie_gbs": pred_bytes * info.pred_size * a.steps * len(roots) / max(e2e_t - e2e_dev, 1e-9) / 1e9},
         "gpu_launches": rec["launches"],
         "roofline": {"bound": "hbm", "kernel": "bfs_persistent_kernel", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_per_bfs(a),
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic_per_launch("bfs_persistent_kernel", a.scale)[0],
+                     "traffic_source": traffic_per_launch("bfs_persistent_kernel", a.scale)[1],
                      "bytes_per_launch": bytes_per_bfs, "ms_per_launch": ms_per_bfs,
                      "bytes_split": {"pred": rec["pred_bytes"] / runs, "top_down": rec["td_bytes"] / runs,
                                      "bottom_up": rec["bu_bytes"] / runs},
@@ -558,16 +702,8 @@ def our_arm(a):
     line.update(sections)
     if serving is not None:
         line["serving"] = serving
-    if world == 1 and not a.no_cpu_baseline:
-        crec, err = run_ref_bench(a.scale, a.edgefactor, a.cpu_roots, 0, 1, a.cpu_roots, a.reorder)
-        if crec is not None:
-            runs = crec["runs"]
-            cv = sum(x[3] for x in runs) / sum(x[2] for x in runs) / 1e9
-            line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": crec["cores"], "kind": "reference",
-                                    "sample": f"{len(runs)} roots of the reference run_bfs at SCALE {a.scale} "
-                                              f"(same graph), OMP {crec['cores']} threads, {cpu_model()}"}
-        else:
-            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": err}
+    if a.scale in cpu:
+        line["cpu_baseline"] = cpu[a.scale]
     print(json.dumps(line))
     bfs.close()
     if dist:

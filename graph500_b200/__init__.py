@@ -81,7 +81,7 @@ class MsTune(C.Structure):
 
 class MsLevel(C.Structure):
     _fields_ = [("level", C.c_int32), ("pull", C.c_int32), ("discovered", C.c_int64), ("device_ms", C.c_double),
-                ("expand_ms", C.c_double)]
+                ("expand_ms", C.c_double), ("rows_read", C.c_int64), ("sectors", C.c_int64)]
 
 
 class ServerConfig(C.Structure):
@@ -181,6 +181,7 @@ def lib() -> C.CDLL:
         "g500_msbfs_wait": ([P, C.POINTER(MsStats)], i32),
         "g500_msbfs_set_root_stats": ([P, i32], i32),
         "g500_msbfs_set_grid": ([P, i32], i32),
+        "g500_msbfs_set_count": ([P, i32], i32),
         "g500_msbfs_get_grid": ([P, i32, C.POINTER(i32), C.POINTER(i32)], i32),
         "g500_msbfs_workspace_bytes": ([P, C.POINTER(u64)], i32),
         "g500_selftest_barrier_timeout": ([i32, C.POINTER(i32), C.POINTER(i32)], i32),
@@ -542,6 +543,10 @@ class MultiSourceBFS:
 
     def set_root_stats(self, on: bool = True) -> None:
         check(lib().g500_msbfs_set_root_stats(self.h, int(on)))
+
+    def set_count(self, on: bool = True) -> None:
+        """Counting runs: level_info() then carries rows_read and sectors per level (untimed use)."""
+        check(lib().g500_msbfs_set_count(self.h, int(on)))
 
     def set_grid(self, blocks: int = 0) -> None:
         check(lib().g500_msbfs_set_grid(self.h, blocks))

@@ -125,13 +125,17 @@ __device__ __forceinline__ void flush_counter(unsigned long long* c, unsigned lo
 // chunks are not left to one lane; a row of more than BIG_CHUNKS chunks is
 // listed whole instead (while the list has room), for the next top-down
 // level to spread over every warp.
+// The warp's items and the listed rows are added to *items / *bigs (lane 0
+// counts the items, each listing lane its row) for the phase's totals.
 __device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t orig, TdItem* __restrict__ q_out,
                                            int64_t cap, unsigned long long* qcount, BfsCtl* ctl, TdItem* big,
-                                           unsigned long long* bigcount) {
+                                           unsigned long long* bigcount, unsigned long long* items,
+                                           unsigned long long* bigs) {
   const int lane = threadIdx.x & 31;
   uint32_t nch = chunks_of(deg);
   if (nch > BIG_CHUNKS && deg < (1ull << 31)) {
     const unsigned long long bi = atomicAdd(bigcount, 1ull);
+    ++*bigs;
     if (bi < (unsigned long long)BIG_ROWS) {
       TdItem it;
       it.begin = rb;
@@ -144,6 +148,7 @@ __device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t o
   const uint32_t incl = warp_incl_scan(nch);
   const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
   if (total == 0) return;
+  if (lane == 0) *items += total;
   const uint32_t excl = incl - nch;
   unsigned long long base = 0;
   if (lane == 31) base = atomicAdd(qcount, (unsigned long long)total);
@@ -180,7 +185,7 @@ __device__ __forceinline__ void append_row(uint64_t rb, uint64_t deg, uint32_t o
 // a prefix of their chunk counts that each block keeps in shared memory.
 template <int DEF>
 __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, int64_t qn, int64_t nbig, uint32_t* vis,
-                         uint2* __restrict__ found_list, unsigned long long* cnt, unsigned long long* sh_acc,
+                         uint2* __restrict__ found_list, unsigned long long* pos, unsigned long long* sh_acc,
                          int64_t lvl) {
   __shared__ uint32_t sh_bigpre[BIG_ROWS + 1];  // sh_bigpre[i] = chunks of big rows 0 .. i-1
   const int lane = threadIdx.x & 31;
@@ -276,7 +281,7 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
       const uint32_t wtotal = __shfl_sync(FULL_MASK, wincl, 31);
       if (wtotal) {
         unsigned long long fb = 0;
-        if (lane == 31) fb = atomicAdd(&cnt[C_QITEMS], (unsigned long long)wtotal);
+        if (lane == 31) fb = atomicAdd(&pos[P_ITEMS], (unsigned long long)wtotal);
         fb = __shfl_sync(FULL_MASK, fb, 31) + wincl - nwon;
 #pragma unroll
         for (int j = 0; j < TD_UNROLL; ++j)
@@ -286,6 +291,7 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
     }
   }
   block_add(sh_acc, C_DISC, found);
+  block_add(sh_acc, C_QITEMS, found);  // every find is listed
   block_add(sh_acc, C_MF, mf);
   if (p.count_edges) {
     block_add(sh_acc, C_FRONT, frontier);
@@ -296,9 +302,9 @@ __device__ void td_phase(const RunParams& p, const TdItem* __restrict__ q_in, in
 
 // Top-down -> top-down: the listed vertices' rows become work items.
 __device__ void chunk_phase(const RunParams& p, const uint2* __restrict__ found_list, int64_t n, TdItem* q_out,
-                            unsigned long long* cnt, unsigned long long* sh_acc) {
+                            unsigned long long* pos, unsigned long long* sh_acc) {
   const int lane = threadIdx.x & 31;
-  unsigned long long skipped = 0;
+  unsigned long long skipped = 0, items = 0, bigs = 0;
   for (int64_t base = gwarp_id() * 32; base < n; base += gwarp_count() * 32) {
     const int64_t i = base + lane;
     uint64_t rb = 0, deg = 0;
@@ -311,9 +317,11 @@ __device__ void chunk_phase(const RunParams& p, const uint2* __restrict__ found_
       skipped += (deg < 2);
       if (deg < 2) deg = 0;  // a degree-1 vertex only leads back to its parent
     }
-    append_row(rb, deg, ow, q_out, p.cap, &cnt[C_QITEMS], p.ctl, p.big, &cnt[C_BIG]);
+    append_row(rb, deg, ow, q_out, p.cap, &pos[P_ITEMS], p.ctl, p.big, &pos[P_BIG], &items, &bigs);
   }
   block_add(sh_acc, C_SKIP, skipped);
+  block_add(sh_acc, C_QITEMS, items);
+  block_add(sh_acc, C_BIG, bigs);
 }
 
 __device__ __forceinline__ bool vis_test(const uint32_t* __restrict__ vis, uint32_t v) {
@@ -477,10 +485,10 @@ __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cu
 // Bottom-up -> top-down: vertices found by the last bottom-up level
 // (vis_new & ~vis_old) become work items.
 __device__ void compact_phase(const RunParams& p, const uint32_t* __restrict__ vis_new,
-                              const uint32_t* __restrict__ vis_old, TdItem* q_out, unsigned long long* cnt,
+                              const uint32_t* __restrict__ vis_old, TdItem* q_out, unsigned long long* pos,
                               unsigned long long* sh_acc) {
   const int lane = threadIdx.x & 31;
-  unsigned long long skipped = 0;
+  unsigned long long skipped = 0, items = 0, bigs = 0;
   for (int64_t wbase = gwarp_id() * 32; wbase < p.nwords; wbase += gwarp_count() * 32) {
     const int64_t wi = wbase + lane;
     const uint32_t f = wi < p.nwords ? (__ldcg(vis_new + wi) & ~__ldcg(vis_old + wi)) : 0u;
@@ -499,10 +507,12 @@ __device__ void compact_phase(const RunParams& p, const uint32_t* __restrict__ v
         skipped += (deg < 2);
         if (deg < 2) deg = 0;
       }
-      append_row(rb, deg, ow, q_out, p.cap, &cnt[C_QITEMS], p.ctl, p.big, &cnt[C_BIG]);
+      append_row(rb, deg, ow, q_out, p.cap, &pos[P_ITEMS], p.ctl, p.big, &pos[P_BIG], &items, &bigs);
     }
   }
   block_add(sh_acc, C_SKIP, skipped);
+  block_add(sh_acc, C_QITEMS, items);
+  block_add(sh_acc, C_BIG, bigs);
 }
 
 __device__ __forceinline__ void write_record(LevelRecord* rec, int level, bool td, unsigned long long frontier,
@@ -551,6 +561,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   for (int64_t i = tid; i < p.nwords; i += nthreads)
     p.vis[0][i] = p.vis_init[i] | (has_edges && i == (int64_t)(root_r >> 5) ? 1u << (root_r & 31) : 0u);
   if (blockIdx.x == 0 && threadIdx.x < 3 * C_NUM) (&ctl->cnt[0][0])[threadIdx.x] = 0;
+  if (blockIdx.x == 0 && threadIdx.x < 3 * P_NUM) (&ctl->pos[0][0])[threadIdx.x] = 0;
 
   // first_expand (bfs.hpp:477-518): the root's row becomes the first queue
   for (int64_t c = tid; c < root_items; c += nthreads) {
@@ -579,11 +590,13 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   int64_t mu = (int64_t)(p.off[p.nlv] - root_deg);  // degree sum of unvisited vertices (edge policy)
   unsigned phase = 0;
   int level = 1;
-  // Each phase uses counter slot phase%3 and clears slot (phase+1)%3 for the
-  // next one; a slot is read right after its phase's barrier, so it is never
-  // cleared while a block may still read it.
+  // Each phase uses counter and position slot phase%3 and clears slot
+  // (phase+1)%3 for the next one; a slot is read right after its phase's
+  // barrier, so it is never cleared while a block may still read it, and it
+  // is cleared before any block can arrive at the barrier that sums into it.
 #define NEXT_PHASE_SLOT()                                                              \
   (blockIdx.x == 0 && threadIdx.x < C_NUM ? (void)(ctl->cnt[(phase + 1) % 3][threadIdx.x] = 0) : (void)0), \
+  (blockIdx.x == 0 && threadIdx.x < P_NUM ? (void)(ctl->pos[(phase + 1) % 3][threadIdx.x] = 0) : (void)0), \
       ctl->cnt[phase % 3]
   for (;; ++level) {
     if (DEF == 2 && level >= PACK_LEVELS) {  // the packed level field is full: the host reruns unpacked
@@ -594,8 +607,8 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
     const int64_t lvl = (int64_t)level << 48;
     unsigned long long disc, scan = 0, edges, sect, front = 0, listed = 0, t_mid = 0, mf = 0;
     if (forward) {
-      td_phase<DEF>(p, items, qn, nbig, p.vis[cur_vis], found_list, cnt, sh_acc, lvl);
-      if (!grid_sync<C_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
+      td_phase<DEF>(p, items, qn, nbig, p.vis[cur_vis], found_list, ctl->pos[phase % 3], sh_acc, lvl);
+      if (!grid_sync_sum<C_NUM>(cnt, &ctl->bar, sh_acc, sh_cnt)) return;
       if (tid == 0) t_mid = globaltimer();
       ++phase;
       disc = sh_cnt[C_DISC];
@@ -606,7 +619,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
       mf = sh_cnt[C_MF];
     } else {
       bu_level<DEF>(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], sh_acc, lvl);
-      if (!grid_sync<C_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
+      if (!grid_sync_sum<C_NUM>(cnt, &ctl->bar, sh_acc, sh_cnt)) return;
       if (tid == 0) t_mid = globaltimer();
       ++phase;
       disc = sh_cnt[C_DISC];
@@ -646,9 +659,9 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
     prev_nq = nq;
     if (forward) {
       unsigned long long* ccnt = (NEXT_PHASE_SLOT());
-      if (was_forward) chunk_phase(p, found_list, (int64_t)listed, items, ccnt, sh_acc);
-      else compact_phase(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], items, ccnt, sh_acc);
-      if (!grid_sync<C_NUM>(&ctl->bar, ccnt, sh_acc, ccnt, sh_cnt, &sh_flag)) return;
+      if (was_forward) chunk_phase(p, found_list, (int64_t)listed, items, ctl->pos[phase % 3], sh_acc);
+      else compact_phase(p, p.vis[cur_vis], p.vis[cur_vis ^ 1], items, ctl->pos[phase % 3], sh_acc);
+      if (!grid_sync_sum<C_NUM>(ccnt, &ctl->bar, sh_acc, sh_cnt)) return;
       ++phase;
       qn = (int64_t)sh_cnt[C_QITEMS];
       nbig = (int64_t)(sh_cnt[C_BIG] < (unsigned long long)BIG_ROWS ? sh_cnt[C_BIG] : (unsigned long long)BIG_ROWS);

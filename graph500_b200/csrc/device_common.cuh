@@ -143,4 +143,52 @@ __device__ bool grid_sync(GridBarrier* bar, unsigned long long* flush_slot, unsi
   return *sh_flag != 0;
 }
 
+// Grid-wide barrier that also sums NC block counters, for a cooperative
+// launch of fewer than 65536 blocks.  The counters ride on the arrivals:
+// thread i < NC of every block adds (sh_acc[i] << 16) | 1 to slot[i] with
+// release semantics (fire and forget), then polls slot[i] until its low 16
+// bits count every block; the high 48 bits are then the grid's sum, copied to
+// sh_cnt[i].  One reduction per counter instead of a reduction, an arrival
+// and a read-back in turn: 2.1 us per barrier on 296 blocks of a B200 against
+// 3.4 us for grid_sync with counters.  The NC words of slot must be zero
+// before the first block arrives and stay untouched until every block has
+// passed (the kernels rotate three slots and clear the next one a phase
+// ahead).  Polls are bounded like grid_sync's; on timeout or an error raised
+// elsewhere while a block waits, every block returns false.  An error raised
+// before a barrier that still completes is not reported by it (that would
+// cost one more round trip per barrier): the kernels decide to stop from the
+// sums themselves (queue overflow, depth), and a block that gives up returns
+// before arriving, so that the others time out or see the flag in their polls.
+template <int NC>
+__device__ bool grid_sync_sum(unsigned long long* slot, GridBarrier* bar, unsigned long long* sh_acc,
+                              unsigned long long* sh_cnt, unsigned long long spin_limit = SPIN_LIMIT) {
+  __syncthreads();
+  bool fail = false;
+  if (threadIdx.x < NC) {
+    unsigned long long* w = slot + threadIdx.x;
+    const unsigned long long v = (sh_acc[threadIdx.x] << 16) | 1ull;
+    sh_acc[threadIdx.x] = 0;
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(w), "l"(v) : "memory");
+    volatile const unsigned long long* vw = w;
+    volatile const unsigned* err = &bar->err;
+    unsigned long long x, spins = 0;
+    while (((x = *vw) & 0xFFFFull) != (unsigned long long)gridDim.x) {
+      ++spins;
+      if ((spins & 15) == 0 && *err) {
+        fail = true;
+        break;
+      }
+      if (spins > spin_limit) {
+        atomicOr(&bar->err, (unsigned)GRID_ERR_TIMEOUT);
+        fail = true;
+        break;
+      }
+      __nanosleep(32);
+    }
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+    sh_cnt[threadIdx.x] = x >> 16;
+  }
+  return !__syncthreads_or(fail);
+}
+
 }  // namespace g500

@@ -140,9 +140,14 @@ struct GridBarrier {
   unsigned pad;
 };
 
+// Append positions of a phase (found list / work items, listed long rows),
+// three rotating slots like the counters
+enum BfsPos { P_ITEMS = 0, P_BIG, P_NUM };
+
 // Control block of one run, in device memory.
 struct BfsCtl {
   unsigned long long cnt[3][C_NUM];
+  unsigned long long pos[3][P_NUM];
   GridBarrier bar;
   unsigned num_levels;
   int final_vis;

@@ -33,7 +33,9 @@ constexpr int MS_THREADS = 256;
 constexpr int MS_MIN_BLOCKS = 4;
 constexpr int MS_MAX_LANES = 128;
 constexpr int MS_MAX_LEVEL = 254;  // level bytes: 255 marks unreached
-enum MsCounter { M_NEW = 0, M_NF, M_MF, M_MU, M_EDGES, M_NUM = 8 };
+// M_ROWS / M_SECT (counting launches only): row and chunk offset reads, and
+// the 32-byte adjacency sectors the level's entries span
+enum MsCounter { M_NEW = 0, M_NF, M_MF, M_MU, M_EDGES, M_ROWS, M_SECT, M_NUM = 8 };
 enum MsErr { MS_ERR_DEPTH = 4 };
 
 struct MsCtl {
@@ -48,6 +50,8 @@ struct MsCtl {
   unsigned long long level_t_ns[MS_MAX_LEVEL + 2];
   unsigned long long level_mid_ns[MS_MAX_LEVEL + 2];  // end of the pull/push phase
   unsigned char level_pull[MS_MAX_LEVEL + 2];
+  unsigned long long level_rows[MS_MAX_LEVEL + 2];  // counting launches: offset reads of the level
+  unsigned long long level_sect[MS_MAX_LEVEL + 2];  // counting launches: adjacency sectors of the level
 };
 
 struct MsParams {
@@ -176,13 +180,19 @@ __device__ __forceinline__ void write_levels(uint8_t* row, const Mask<NW>& nw, c
   }
 }
 
+// 32-byte sectors spanned by the k adjacency entries (4 bytes each) at b
+__device__ __forceinline__ unsigned long long sector_span(uint64_t b, uint64_t k) {
+  return k ? ((b + k - 1) >> 3) - (b >> 3) + 1 : 0;
+}
+
 // Per-thread counters of a level, flushed once per block at its end.
 template <int NW>
 struct LevelAcc {
   unsigned long long nnew, nf, mf, mu;
+  unsigned long long rows, sect;  // counting launches only
   Mask<NW> lanes;  // lanes that found vertices
   __device__ void clear() {
-    nnew = nf = mf = mu = 0;
+    nnew = nf = mf = mu = rows = sect = 0;
 #pragma unroll
     for (int k = 0; k < NW; ++k) lanes.w[k] = 0;
   }
@@ -231,7 +241,7 @@ __device__ __forceinline__ void settle(const MsParams& p, uint32_t* Fn, int64_t 
 // INTO_N (a level that pulls some lanes and pushes the others): a row's
 // finds go into its next mask N, beside the push's, for the apply pass to
 // settle, instead of settling here.
-template <int NW, bool INTO_N>
+template <int NW, bool INTO_N, bool COUNT>
 __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, const uint32_t* Fc, uint32_t* Fn,
                              uint32_t lvl4, LevelAcc<NW>& la) {
   const int lane = threadIdx.x & 31;
@@ -261,7 +271,8 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, const uint3
     }
     if (any && deg <= (uint32_t)MS_SMALL_DEG) {
       const uint64_t re = rb + deg;
-      for (uint64_t e = rb; e < re; e += MS_UNROLL) {
+      uint64_t e = rb;
+      for (; e < re; e += MS_UNROLL) {
         uint32_t nb[MS_UNROLL];
 #pragma unroll
         for (int t = 0; t < MS_UNROLL; ++t) nb[t] = e + t < re ? __ldg(p.col + e + t) : NO_VERTEX;
@@ -273,6 +284,11 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, const uint3
             for (int q = 0; q < NW; ++q) acc.w[q] |= f.w[q];
           }
         if (covers<NW>(acc, need)) break;
+      }
+      if constexpr (COUNT) {
+        const uint64_t k = (e + MS_UNROLL < re ? e + MS_UNROLL : re) - rb;
+        ++la.rows;
+        la.sect += sector_span(rb, k);
       }
     }
     unsigned rows = __ballot_sync(FULL_MASK, any && deg > (uint32_t)MS_SMALL_DEG && deg <= (uint32_t)MS_HUB_DEG);
@@ -287,7 +303,8 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, const uint3
         nd.w[k] = __shfl_sync(FULL_MASK, need.w[k], src);
         a.w[k] = 0;
       }
-      for (uint64_t j = b; j < e; j += 32 * MS_UNROLL) {
+      uint64_t j = b;
+      for (; j < e; j += 32 * MS_UNROLL) {
         uint32_t nb[MS_UNROLL];
 #pragma unroll
         for (int t = 0; t < MS_UNROLL; ++t) {
@@ -308,7 +325,13 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, const uint3
         for (int k = 0; k < NW; ++k) a.w[k] |= __reduce_or_sync(FULL_MASK, x.w[k]);
         if (covers<NW>(a, nd)) break;
       }
-      if (lane == src) acc = a;
+      if (lane == src) {
+        acc = a;
+        if constexpr (COUNT) {
+          ++la.rows;
+          la.sect += sector_span(b, (j + 32 * MS_UNROLL < e ? j + 32 * MS_UNROLL : e) - b);
+        }
+      }
     }
     // hub rows settle after the hub phase (deg is 0 here for rows without needed lanes)
     if (v < p.nlv && deg <= (uint32_t)MS_HUB_DEG) {
@@ -343,8 +366,8 @@ __device__ __forceinline__ void hub_bounds(const MsParams& p, uint32_t h, uint32
 
 // pull over hub rows: each chunk ORs its neighbours' frontier masks, stopping
 // once the row's unvisited lanes are covered, into the row's next mask
-template <int NW>
-__device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act, const uint32_t* Fc) {
+template <int NW, bool COUNT>
+__device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act, const uint32_t* Fc, LevelAcc<NW>& la) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = gwarp_count();
   for (int64_t c0 = gwarp_id(); c0 < p.nhub_chunks; c0 += 32 * nwarps) {
@@ -377,7 +400,8 @@ __device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act, const uint3
       }
       uint64_t b, e;
       hub_bounds<MS_HUB_CHUNK>(p, h, kk, &b, &e);
-      for (uint64_t j = b; j < e; j += 32 * MS_UNROLL) {
+      uint64_t j = b;
+      for (; j < e; j += 32 * MS_UNROLL) {
         uint32_t nb[MS_UNROLL];
 #pragma unroll
         for (int t = 0; t < MS_UNROLL; ++t) {
@@ -398,6 +422,11 @@ __device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act, const uint3
         for (int k = 0; k < NW; ++k) a.w[k] |= __reduce_or_sync(FULL_MASK, x.w[k]);
         if (covers<NW>(a, nd)) break;
       }
+      if constexpr (COUNT)
+        if (lane == 0) {
+          ++la.rows;
+          la.sect += sector_span(b, (j + 32 * MS_UNROLL < e ? j + 32 * MS_UNROLL : e) - b);
+        }
       if (lane < NW) {
         uint32_t x = 0;
 #pragma unroll
@@ -411,8 +440,8 @@ __device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act, const uint3
 
 // push from hub frontier rows: every neighbour of the chunk gets the lanes it
 // still lacks
-template <int NW>
-__device__ void ms_push_hubs(const MsParams& p, const uint32_t* Fc, const Mask<NW>& qm) {
+template <int NW, bool COUNT>
+__device__ void ms_push_hubs(const MsParams& p, const uint32_t* Fc, const Mask<NW>& qm, LevelAcc<NW>& la) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = gwarp_count();
   for (int64_t c0 = gwarp_id(); c0 < p.npush_chunks; c0 += 32 * nwarps) {
@@ -442,6 +471,11 @@ __device__ void ms_push_hubs(const MsParams& p, const uint32_t* Fc, const Mask<N
       for (int k = 0; k < NW; ++k) fo.w[k] = __shfl_sync(FULL_MASK, f.w[k], src);
       uint64_t b, e;
       hub_bounds<MS_PUSH_CHUNK>(p, h, kk, &b, &e);
+      if constexpr (COUNT)
+        if (lane == 0) {
+          ++la.rows;
+          la.sect += sector_span(b, e - b);
+        }
       for (uint64_t j = b; j < e; j += 32 * MS_UNROLL) {
         uint32_t nb[MS_UNROLL];
 #pragma unroll
@@ -468,8 +502,8 @@ __device__ void ms_push_hubs(const MsParams& p, const uint32_t* Fc, const Mask<N
 // 32 rows are loaded together; each group holding frontier rows has their
 // edges walked as one list, MS_WIN at a time; every neighbour gets the lanes
 // it still lacks.
-template <int NW>
-__device__ void ms_push_rows(const MsParams& p, const uint32_t* Fc, const Mask<NW>& qm) {
+template <int NW, bool COUNT>
+__device__ void ms_push_rows(const MsParams& p, const uint32_t* Fc, const Mask<NW>& qm, LevelAcc<NW>& la) {
   const int lane = threadIdx.x & 31;
   for (int64_t base = gwarp_id() * (32 * MS_GROUPS); base < p.nlv; base += gwarp_count() * (32 * MS_GROUPS)) {
     Mask<NW> fg[MS_GROUPS];
@@ -498,6 +532,11 @@ __device__ void ms_push_rows(const MsParams& p, const uint32_t* Fc, const Mask<N
         cur = __ldg(p.off + v);
         re = cur + __ldg(p.deg + v);
         if (re - cur > (uint64_t)MS_PUSH_HUB_DEG) cur = re;  // hub row: the hub phase pushes it
+        if constexpr (COUNT)
+          if (re > cur) {
+            ++la.rows;
+            la.sect += sector_span(cur, re - cur);
+          }
       }
       for (;;) {
         const uint32_t rem = (uint32_t)((re - cur) < (uint64_t)MS_WIN ? (re - cur) : (uint64_t)MS_WIN);
@@ -650,9 +689,13 @@ __device__ void ms_lane_survey(const MsParams& p, const uint32_t* Fc, unsigned l
 
 // the level's counters into the block accumulators, and the lanes that found
 // vertices (the others have finished their BFS) into alive_out
-template <int NW>
+template <int NW, bool COUNT>
 __device__ void flush_level(const LevelAcc<NW>& la, unsigned long long* sh_acc, unsigned* sh_or,
                             unsigned* alive_out) {
+  if constexpr (COUNT) {
+    block_add(sh_acc, M_ROWS, la.rows);
+    block_add(sh_acc, M_SECT, la.sect);
+  }
   block_add(sh_acc, M_NEW, la.nnew);
   block_add(sh_acc, M_NF, la.nf);
   block_add(sh_acc, M_MF, la.mf);
@@ -669,7 +712,10 @@ __device__ void flush_level(const LevelAcc<NW>& la, unsigned long long* sh_acc, 
   }
 }
 
-template <int NW>
+// COUNT: a counting launch, which also records each level's offset reads and
+// adjacency sectors (the bytes model of the batched form); compiled apart so
+// that the timed launches carry none of it.
+template <int NW, bool COUNT>
 __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsParams p) {
   constexpr int W = 32 * NW;
   __shared__ unsigned long long sh_cnt[M_NUM];
@@ -774,16 +820,16 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
       for (int k = 0; k < NW; ++k) mixed |= qm.w[k] != 0;
     }
     if (pull && !mixed) {
-      ms_pull_rows<NW, false>(p, act, Fc, Fn, lvl4, la);
-      ms_pull_hubs<NW>(p, act, Fc);
+      ms_pull_rows<NW, false, COUNT>(p, act, Fc, Fn, lvl4, la);
+      ms_pull_hubs<NW, COUNT>(p, act, Fc, la);
     } else if (mixed) {
-      ms_push_rows<NW>(p, Fc, qm);
-      ms_push_hubs<NW>(p, Fc, qm);
-      ms_pull_rows<NW, true>(p, pm, Fc, Fn, lvl4, la);
-      ms_pull_hubs<NW>(p, pm, Fc);
+      ms_push_rows<NW, COUNT>(p, Fc, qm, la);
+      ms_push_hubs<NW, COUNT>(p, Fc, qm, la);
+      ms_pull_rows<NW, true, COUNT>(p, pm, Fc, Fn, lvl4, la);
+      ms_pull_hubs<NW, COUNT>(p, pm, Fc, la);
     } else {
-      ms_push_rows<NW>(p, Fc, qm);
-      ms_push_hubs<NW>(p, Fc, qm);
+      ms_push_rows<NW, COUNT>(p, Fc, qm, la);
+      ms_push_hubs<NW, COUNT>(p, Fc, qm, la);
     }
     pulls += pull;
     if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
@@ -794,14 +840,18 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
       for (int i = threadIdx.x; i < MS_MAX_LANES; i += blockDim.x) ctl->lane_deg[i] = 0;
     if (pull && !mixed) ms_settle_hubs<NW>(p, act, Fn, lvl4, la);
     else ms_apply<NW>(p, act, Fn, lvl4, la);
-    flush_level<NW>(la, sh_acc, sh_or, alive);
-    if (!grid_sync<M_NUM>(&ctl->bar, cnt, sh_acc, cnt, sh_cnt, &sh_flag)) return;
+    flush_level<NW, COUNT>(la, sh_acc, sh_or, alive);
+    if (!grid_sync_sum<M_NUM>(cnt, &ctl->bar, sh_acc, sh_cnt)) return;
     ++phase;
     const unsigned long long nnew = sh_cnt[M_NEW];
     if (tid == 0) {
       ctl->level_new[level] = nnew;
       ctl->level_t_ns[level] = globaltimer();
       ctl->level_pull[level] = pull ? (mixed ? 2 : 1) : 0;
+      if constexpr (COUNT) {
+        ctl->level_rows[level] = sh_cnt[M_ROWS];
+        ctl->level_sect[level] = sh_cnt[M_SECT];
+      }
     }
     // a lane that found nothing this level has finished: it no longer needs anything
     {
@@ -992,6 +1042,7 @@ struct g500_msbfs {
   int lane_width = 64;
   double alpha = 15.0;
   int use_graph = 1;
+  int count = 0;                    // counting launches (no CUDA graph): per-level offset reads and sectors
   unsigned grid[3] = {0, 0, 0};     // co-resident blocks per lane width (NW = 1, 2, 4)
 
   uint32_t *V = nullptr, *F = nullptr, *N = nullptr;  // [nlv][4] words (room for 128 lanes)
@@ -1063,7 +1114,7 @@ static int ms_free(g500_msbfs* m) {
 }
 
 template <int NW>
-static const void* ms_kernel_ptr() { return (const void*)msbfs_kernel<NW>; }
+static const void* ms_kernel_ptr() { return (const void*)msbfs_kernel<NW, false>; }
 
 // Chunk table of the rows longer than `thresh`, `chunk` edges per chunk, so
 // that warps can share a hub's row.
@@ -1170,9 +1221,15 @@ static int ms_enqueue_batch(g500_msbfs* m, int b, cudaStream_t s) {
   attr.val.cooperative = 1;
   cfg.attrs = &attr;
   cfg.numAttrs = 1;
-  if (W == 32) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<1>, p));
-  else if (W == 64) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<2>, p));
-  else G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<4>, p));
+  if (m->count) {  // the counting variant has the timed kernel's grid (same launch bounds)
+    if (W == 32) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<1, true>, p));
+    else if (W == 64) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<2, true>, p));
+    else G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<4, true>, p));
+  } else {
+    if (W == 32) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<1, false>, p));
+    else if (W == 64) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<2, false>, p));
+    else G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<4, false>, p));
+  }
   uint8_t* out = m->out + (int64_t)b * W * g->nolv;
   const unsigned tg = (unsigned)std::min<int64_t>(ceil_div(g->nolv, 4 * TR_BLOCK), (int64_t)num_sms() * 8);
   if (W == 32) ms_transpose_kernel<1><<<tg, TR_BLOCK, 0, s>>>(m->L, m->V, g->d_reorder, g->nlv, g->nolv, m->nroots_dev + b, out);
@@ -1295,7 +1352,7 @@ static int ms_launch(g500_msbfs* m, const int64_t* roots, int nroots, uint8_t* l
   cudaStream_t s = m->stream;
   G500_CUDA(cudaEventRecord(m->ev0, s));
   for (int b = 0; b < batches; ++b) {
-    if (m->use_graph) {
+    if (m->use_graph && !m->count) {
       if (!m->graphs[ni][b]) {
         cudaGraph_t graph = nullptr;
         G500_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1491,7 +1548,16 @@ extern "C" int g500_msbfs_level_info(const g500_msbfs* m, int batch, g500_msbfs_
     const unsigned long long prev = l == 1 ? c.t_init_ns : c.level_t_ns[l - 1];
     r.device_ms = c.level_t_ns[l] >= prev ? (double)(c.level_t_ns[l] - prev) * 1e-6 : 0.0;
     r.expand_ms = c.level_mid_ns[l] >= prev ? (double)(c.level_mid_ns[l] - prev) * 1e-6 : 0.0;
+    r.rows_read = m->count ? (int64_t)c.level_rows[l] : -1;
+    r.sectors = m->count ? (int64_t)c.level_sect[l] : -1;
   }
+  return G500_OK;
+}
+
+extern "C" int g500_msbfs_set_count(g500_msbfs* m, int on) {
+  if (!m) return set_error(G500_E_INVAL, "null argument");
+  if (m->in_flight) return set_error(G500_E_STATE, "a launch is in flight");
+  m->count = on ? 1 : 0;
   return G500_OK;
 }
 

@@ -282,10 +282,16 @@ typedef struct g500_msbfs_level {
   int64_t discovered;      /* new (vertex, lane) pairs */
   double device_ms;        /* the whole level */
   double expand_ms;        /* its pull or push phase (the rest is the apply pass) */
+  int64_t rows_read;       /* counting runs: row (or hub chunk) offset reads of the level, else -1 */
+  int64_t sectors;         /* counting runs: 32-byte adjacency sectors the level's examined entries span, else -1 */
 } g500_msbfs_level;
 /* Copies up to max_levels records of launch `batch` of the last run into out;
  * *num_levels receives the launch's level count. */
 int g500_msbfs_level_info(const g500_msbfs* m, int batch, g500_msbfs_level* out, int max_levels, int* num_levels);
+/* on != 0: later runs are counting runs (a kernel variant that also records
+ * each level's rows_read and sectors for the bytes model, launched without
+ * the CUDA graph); their levels are the same.  Meant for untimed runs. */
+int g500_msbfs_set_count(g500_msbfs* m, int on);
 /* Asynchronous form of g500_msbfs_run for callers that overlap several
  * handles (the serving loop): launch enqueues the whole call on the handle's
  * stream and returns; poll reports whether it finished; wait blocks until it

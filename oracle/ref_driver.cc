@@ -145,16 +145,21 @@ REF_API void ref_release() {
 #ifdef G500_REF_MAIN
 /*
  * Stand-alone bounded benchmark of the reference path:
- *   ref_bench SCALE EDGEFACTOR NROOTS WARMUP STEPS ROOTS_PER_STEP
+ *   ref_bench SCALE EDGEFACTOR NROOTS WARMUP STEPS ROOTS_PER_STEP [gate]
  * Generation, construction and validation are untimed; each step runs
  * ROOTS_PER_STEP consecutive roots (cycling over the NROOTS find_roots roots)
  * and reports per-root BFS wall times.  Output: one JSON object on stdout.
+ * With "gate", the process prints "ready" on stdout once the graph is built
+ * and validated, and starts the timed runs only when a line arrives on stdin
+ * (so that a caller can overlap construction with other work and time the
+ * runs alone); an empty stdin (EOF) ends it without timing.
  */
 int main(int argc, char** argv) {
   if (argc < 7) {
-    fprintf(stderr, "usage: %s SCALE EDGEFACTOR NROOTS WARMUP STEPS ROOTS_PER_STEP\n", argv[0]);
+    fprintf(stderr, "usage: %s SCALE EDGEFACTOR NROOTS WARMUP STEPS ROOTS_PER_STEP [gate]\n", argv[0]);
     return 2;
   }
+  const bool gate = argc > 7 && strcmp(argv[7], "gate") == 0;
   int scale = atoi(argv[1]), ef = atoi(argv[2]), nroots = atoi(argv[3]);
   int warmup = atoi(argv[4]), steps = atoi(argv[5]), per_step = atoi(argv[6]);
   double gen = ref_generate(scale, ef);
@@ -171,6 +176,12 @@ int main(int argc, char** argv) {
     double t = MPI_Wtime();
     if (!ref_validate(roots[i], pred, &nedge[i])) { fprintf(stderr, "reference validation failed\n"); return 1; }
     val_time += MPI_Wtime() - t;
+  }
+  if (gate) {
+    printf("ready\n");
+    fflush(stdout);
+    char line[64];
+    if (!fgets(line, sizeof(line), stdin)) return 0;
   }
   int k = 0;
   for (int w = 0; w < warmup; ++w)

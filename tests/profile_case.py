@@ -1,6 +1,7 @@
-"""A small, self-contained run of every kernel on the path, for profilers.
+"""A small, self-contained run of every kernel on the path, for profilers
+(a profiling case kept beside the tests; pytest does not collect it).
 
-    python -m graph500_b200.profile_case SCALE [ALPHA BETA [NROOTS]]
+    python tests/profile_case.py SCALE [ALPHA BETA [NROOTS]]
 
 Generates and builds a Kronecker graph on the GPU (VERTEX_REORDERING 2), runs
 the plain BFS from the first NROOTS find_roots roots with the given direction
@@ -8,7 +9,10 @@ thresholds, validates the last one on the device, and runs one multi-source
 launch over 64 roots (lane width 64, alpha 6, no CUDA graph, so a profiler
 sees each kernel launch).  It prints one line and exits 0.
 """
+import os
 import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 
 
 def main(argv):
