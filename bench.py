@@ -250,6 +250,15 @@ class RefBaselines:
             if not os.path.exists(exe):
                 self.err[scale] = f"{exe} not built"
                 continue
+            # BfsBase::allocate_memory sizes its comm buffer pool as num_local_verts * 4 * 50 bytes and
+            # passes it as an int (mpi/bfs.hpp:173, :283); on one process that overflows from SCALE 25 on
+            # (num_local_verts is about half of 2^SCALE), and the allocation fails (utils.hpp:351)
+            if (1 << scale) * 0.53 * 200 >= 2 ** 31:
+                self.err[scale] = (f"the reference cannot run SCALE {scale} in one process: its comm buffer pool "
+                                   f"size, num_local_verts*4*50 bytes (about {(1 << scale) * 0.49 * 200 / 1e9:.1f} "
+                                   f"GB), is passed as an int (mpi/bfs.hpp:173, :283) and overflows, so its "
+                                   f"allocation fails ('Out of memory trying to allocate', mpi/utils.hpp:351)")
+                continue
             need = self.RAM_GB.get(scale, 4 << max(0, scale - 22))
             have = host_ram_gb()
             if have < need:
@@ -263,7 +272,7 @@ class RefBaselines:
             if line.strip() != "ready":
                 p.wait()
                 log.seek(0)
-                tail = log.read().strip().splitlines()[-1:]
+                tail = log.read().strip().splitlines()[-3:]
                 self.err[scale] = f"ref_bench exit {p.returncode}: {tail}"
                 continue
             self.ready[scale] = (p, log, roots, passes)
@@ -500,14 +509,24 @@ def serving_arm(a, g5, torch, reduce_sum, barrier) -> dict:
     out = {"workload": f"{len(graphs)} resident Kronecker graphs SCALE {'/'.join(map(str, scales))} "
                        f"(edgefactor {a.edgefactor}, VERTEX_REORDERING 2), Poisson arrivals, up to 128 queries "
                        f"per multi-source launch",
-           "queries_per_rate": a.serve_queries, "warmup_queries": a.serve_warmup, "rates": []}
+           "queries_per_rate": a.serve_queries, "warmup_queries": a.serve_warmup}
     srv = g5.Server(graphs, max_batch=128, max_workers_per_graph=a.serve_workers)
     srv.run_poisson(1000.0, 400, seed=7)  # warm-up: captures the CUDA graphs of every lane width in use
-    for rate in [float(x) for x in a.serve_rates.split(",")]:
-        barrier()
-        rep = srv.run_poisson(rate, a.serve_queries + a.serve_warmup, seed=2026, warmup=a.serve_warmup)
-        rep["gteps_all_ranks"] = reduce_sum(rep["gteps"])
-        out["rates"].append(rep)
+    rates = [float(x) for x in a.serve_rates.split(",")]
+    # "rates": each query's levels delivered to a device buffer of its own before it completes;
+    # "rates_no_delivery": completion only (levels left in the launch workspace);
+    # "rates_host_delivery": levels copied to pinned host memory (PCIe-bound), at the rates PCIe can carry
+    out["delivery"] = "device: each query's uint8 level array (pred_size bytes) copied to its own device buffer"
+    for key, mode, rs in (("rates", g5.DELIVER_DEVICE, rates), ("rates_no_delivery", g5.DELIVER_NONE, rates),
+                          ("rates_host_delivery", g5.DELIVER_HOST, [r for r in rates if r <= 3000])):
+        srv.set_delivery(mode)
+        out[key] = []
+        for rate in rs:
+            barrier()
+            rep = srv.run_poisson(rate, a.serve_queries + a.serve_warmup, seed=2026, warmup=a.serve_warmup)
+            rep["gteps_all_ranks"] = reduce_sum(rep["gteps"])
+            out[key].append(rep)
+    srv.set_delivery(g5.DELIVER_NONE)
     out["server"] = srv.info()
     srv.close()
     plain = g5.Server(graphs, mode=g5.SERVE_PLAIN)

@@ -87,7 +87,7 @@ class MsLevel(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("max_batch", C.c_int32), ("max_workers_per_graph", C.c_int32), ("mode", C.c_int32),
                 ("vertices_per_block", C.c_int32), ("hbm_reserve_bytes", C.c_uint64), ("alpha", C.c_double),
-                ("max_grid_fraction", C.c_double), ("plain_below", C.c_int32), ("pad", C.c_int32)]
+                ("max_grid_fraction", C.c_double), ("plain_below", C.c_int32), ("batch_target", C.c_int32)]
 
 
 class QueryResult(C.Structure):
@@ -108,10 +108,11 @@ class ServeReport(C.Structure):
                 ("achieved_qps", C.c_double), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
                 ("mean_ms", C.c_double), ("max_ms", C.c_double), ("gteps", C.c_double), ("nedge", C.c_int64),
                 ("mean_batch", C.c_double), ("launches", C.c_int64), ("max_in_flight", C.c_int32),
-                ("workers", C.c_int32)]
+                ("workers", C.c_int32), ("delivery", C.c_int32), ("pad", C.c_int32)]
 
 
 SERVE_BATCHED, SERVE_PLAIN = 0, 1
+DELIVER_NONE, DELIVER_DEVICE, DELIVER_HOST = 0, 1, 2
 
 
 class ValidateReport(C.Structure):
@@ -193,6 +194,7 @@ def lib() -> C.CDLL:
         "g500_server_info": ([P, C.POINTER(ServerInfo)], i32),
         "g500_server_run_poisson": ([P, C.c_double, i64, u64, i64, C.POINTER(ServeReport)], i32),
         "g500_server_destroy": ([P], i32),
+        "g500_server_set_delivery": ([P, i32], i32),
         "g500_msbfs_autotune": ([P, P, i32, i32, C.POINTER(MsTune)], i32),
         "g500_msbfs_destroy": ([P], i32),
         "g500_validate_noalloc": ([P, i64, i64, i64, i64, P, P, C.POINTER(i64), C.POINTER(i32),
@@ -681,6 +683,10 @@ class Server:
         i = ServerInfo()
         check(lib().g500_server_info(self.h, C.byref(i)))
         return {f[0]: getattr(i, f[0]) for f in ServerInfo._fields_}
+
+    def set_delivery(self, mode: int) -> None:
+        """DELIVER_NONE, DELIVER_DEVICE or DELIVER_HOST for the load generator's queries."""
+        check(lib().g500_server_set_delivery(self.h, int(mode)))
 
     def run_poisson(self, rate_qps: float, num_queries: int, seed: int = 2026, warmup: int = 0) -> dict:
         rep = ServeReport()

@@ -14,7 +14,14 @@
 // (lane width 32/64/128, the smallest that holds them) and launches them
 // asynchronously; queries that arrive meanwhile wait for the next free
 // worker, so batches form from whatever arrived while the device was busy
-// (continuous batching).  Launches of different workers run concurrently on
+// (continuous batching).  Graphs are served oldest waiting query first, and
+// a graph whose launch does not fit in the free blocks reserves them, so that
+// small launches of other graphs cannot starve a large graph (without that,
+// 4 graphs of SCALE 18-24 served only 21k of 30k q/s offered, p99 0.3 s; with
+// it 29.7k, p99 12 ms).  Optionally (batch_target > 0) a second launch of a
+// graph waits until that many of its queries wait; off by default, since it
+// measured worse at 30k q/s (p99 17-62 ms).  Launches of different workers
+// run concurrently on
 // their own streams; the sum of their persistent-kernel grids never exceeds
 // the device's co-resident blocks, so every grid barrier can complete.
 #include "g500_internal.cuh"
@@ -39,6 +46,7 @@ struct Query {
   int graph = 0;
   int64_t root = 0;
   uint8_t* levels_out = nullptr;
+  int slot = -1;          // delivery slot of a load-generator query (g500_server_set_delivery)
   bool internal = false;  // submitted by the load generator: kept out of poll
   g500_query_result res{};
 };
@@ -108,6 +116,12 @@ struct g500_server {
   int64_t* h_pred = nullptr;
   int64_t pred_cap = 0;
 
+  // result delivery of load-generator queries: per graph a ring of level
+  // buffers (device or pinned host memory), one per query in flight
+  int delivery = G500_DELIVER_NONE;
+  std::vector<std::vector<uint8_t*>> slots;   // per graph
+  std::vector<std::vector<int>> free_slots;   // per graph (engine thread)
+
   std::atomic<int64_t> launches{0}, lanes_used{0};
   std::atomic<int> in_flight{0}, max_in_flight{0}, nworkers{0};
   std::thread engine;
@@ -142,6 +156,11 @@ void finish_queries(g500_server* s, const std::vector<int64_t>& qids, int status
       r.done_us = done;
       r.batch_size = batch;
       r.lane_width = lanes;
+      if (it->second.slot >= 0) {
+        s->free_slots[(size_t)it->second.graph].push_back(it->second.slot);
+        it->second.slot = -1;
+        it->second.levels_out = nullptr;
+      }
       if (!it->second.internal) s->completed.push_back(qids[i]);
       ++s->finished;
     }
@@ -211,12 +230,49 @@ bool reap(g500_server* s) {
   return any;
 }
 
+void free_delivery(g500_server* s) {
+  for (auto& gs : s->slots)
+    for (uint8_t* p : gs) {
+      if (s->delivery == G500_DELIVER_HOST) cudaFreeHost(p);
+      else cudaFree(p);
+    }
+  s->slots.clear();
+  s->free_slots.clear();
+  s->delivery = G500_DELIVER_NONE;
+}
+
+// A load-generator query with delivery on gets a free level buffer of its
+// graph as its destination (caller holds s->mu); false when none is free.
+bool take_slot(g500_server* s, int g, Query* q) {
+  if (s->delivery == G500_DELIVER_NONE || !q->internal || q->levels_out) return true;
+  auto& fs = s->free_slots[(size_t)g];
+  if (fs.empty()) return false;
+  q->slot = fs.back();
+  fs.pop_back();
+  q->levels_out = s->slots[(size_t)g][(size_t)q->slot];
+  return true;
+}
+
 // Launch the waiting queries of every graph that has an idle (or admissible
-// new) worker and room in the block budget.
+// new) worker and room in the block budget.  Graphs are served oldest
+// waiting query first.  A graph whose launch does
+// not fit in the free blocks reserves them: graphs behind it may only start
+// launches that leave its share free, so that a large graph's launch is not
+// starved by a stream of small launches of other graphs.
 bool dispatch(g500_server* s) {
   bool any = false;
   const int ng = (int)s->graphs.size();
-  for (int g = 0; g < ng; ++g) {
+  std::vector<std::pair<double, int>> order;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (int g = 0; g < ng; ++g)
+      if (!s->pending[(size_t)g].empty())
+        order.emplace_back(s->queries[s->pending[(size_t)g].front()].res.arrival_us, g);
+  }
+  std::sort(order.begin(), order.end());
+  int reserved = 0;  // blocks kept free for older graphs that could not start
+  for (const auto& og : order) {
+    const int g = og.second;
     for (;;) {
       {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -235,15 +291,20 @@ bool dispatch(g500_server* s) {
             pw = &x;
             break;
           }
-        if (pw && s->inflight_blocks + pw->units <= s->capacity) {
+        if (pw && s->inflight_blocks + pw->units + reserved > s->capacity) {
+          reserved += pw->units;
+          break;
+        }
+        if (pw) {
           int64_t id;
           int64_t root;
           uint8_t* dst;
           {
             std::lock_guard<std::mutex> lk(s->mu);
             id = s->pending[(size_t)g].front();
+            Query& q = s->queries[id];
+            if (!take_slot(s, g, &q)) break;  // every delivery slot is in use: wait for one
             s->pending[(size_t)g].pop_front();
-            const Query& q = s->queries[id];
             root = q.root;
             dst = q.levels_out;
           }
@@ -268,7 +329,16 @@ bool dispatch(g500_server* s) {
         }
         break;  // the plain worker is busy or the budget is full: wait for it
       }
-      if (s->inflight_blocks + s->blocks[(size_t)g] > s->capacity) break;
+      if (s->inflight_blocks + s->blocks[(size_t)g] + reserved > s->capacity) {
+        reserved += s->blocks[(size_t)g];
+        break;
+      }
+      // hold a second launch of this graph until it fills batch_target lanes
+      if (s->cfg.batch_target > 0 && (int)waiting < s->cfg.batch_target) {
+        bool running = false;
+        for (const Worker& x : s->workers[(size_t)g]) running |= x.busy;
+        if (running) break;
+      }
       Worker* w = nullptr;
       for (Worker& x : s->workers[(size_t)g])
         if (!x.busy) {
@@ -299,14 +369,16 @@ bool dispatch(g500_server* s) {
         auto& pq = s->pending[(size_t)g];
         while (!pq.empty() && (int)w->qids.size() < s->cfg.max_batch) {
           const int64_t id = pq.front();
+          Query& q = s->queries[id];
+          if (!take_slot(s, g, &q)) break;
           pq.pop_front();
-          const Query& q = s->queries[id];
           w->qids.push_back(id);
           roots.push_back(q.root);
           dsts.push_back(q.levels_out);
         }
       }
       const int n = (int)roots.size();
+      if (n == 0) break;  // every delivery slot is in use
       const int lanes = n <= 32 ? 32 : (n <= 64 ? 64 : 128);
       int st = g500_msbfs_set_params(w->ms, lanes, s->alpha[(size_t)g], 1);
       w->t_start_us = s->now_us();
@@ -474,6 +546,7 @@ extern "C" int g500_server_default_config(g500_server_config* cfg) {
   cfg->alpha = 6.0;
   cfg->max_grid_fraction = 0.5;
   cfg->plain_below = -1;
+  cfg->batch_target = 0;
   return G500_OK;
 }
 
@@ -666,7 +739,15 @@ extern "C" int g500_server_run_poisson(g500_server* s, double rate_qps, int64_t 
       if (dt <= 0) break;
       if (dt > 200) std::this_thread::sleep_for(std::chrono::microseconds((int64_t)(dt - 100)));
     }
-    G500_TRY(submit_at(s, gs[(size_t)k], rs[(size_t)k], (uint64_t)k, nullptr, at[(size_t)k], true, &ids[(size_t)k]));
+    const int st = submit_at(s, gs[(size_t)k], rs[(size_t)k], (uint64_t)k, nullptr, at[(size_t)k], true,
+                             &ids[(size_t)k]);
+    if (st != G500_OK) {  // let the queries already submitted finish, then forget them
+      const std::string why = g500_last_error();
+      g500_server_drain(s, 600000);
+      std::lock_guard<std::mutex> lk(s->mu);
+      for (int64_t j = 0; j < k; ++j) s->queries.erase(ids[(size_t)j]);
+      return g500::set_error(st, "%s", why.c_str());
+    }
   }
   G500_TRY(g500_server_drain(s, 600000));
   std::vector<double> lat;
@@ -716,6 +797,7 @@ extern "C" int g500_server_run_poisson(g500_server* s, double rate_qps, int64_t 
   rep->mean_batch = rep->launches ? (double)(s->lanes_used.load() - q0) / (double)rep->launches : 0;
   rep->max_in_flight = s->max_in_flight.load();
   rep->workers = s->nworkers.load();
+  rep->delivery = s->delivery;
   return failed ? g500::set_error(G500_E_DEVICE, "%lld queries failed", (long long)failed) : G500_OK;
 }
 
@@ -744,6 +826,39 @@ extern "C" int g500_server_destroy(g500_server* s) {
     if (b) g500_bfs_destroy(b);
   if (s->d_pred) cudaFree(s->d_pred);
   if (s->h_pred) cudaFreeHost(s->h_pred);
+  free_delivery(s);
   delete s;
+  return G500_OK;
+}
+
+extern "C" int g500_server_set_delivery(g500_server* s, int mode) {
+  if (!s) return g500::set_error(G500_E_INVAL, "null handle");
+  if (mode != G500_DELIVER_NONE && mode != G500_DELIVER_DEVICE && mode != G500_DELIVER_HOST)
+    return g500::set_error(G500_E_INVAL, "unknown delivery mode %d", mode);
+  G500_TRY(g500_server_drain(s, 600000));
+  std::lock_guard<std::mutex> lk(s->mu);  // the engine takes slots under this lock
+  free_delivery(s);
+  if (mode == G500_DELIVER_NONE) return G500_OK;
+  G500_CUDA(cudaSetDevice(s->device));
+  const int per_graph = s->cfg.max_batch * s->cfg.max_workers_per_graph + 1;  // + a plain run
+  const size_t ng = s->graphs.size();
+  s->slots.assign(ng, {});
+  s->free_slots.assign(ng, {});
+  for (size_t g = 0; g < ng; ++g) {
+    const size_t bytes = (size_t)std::max<int64_t>(s->graphs[g]->nolv, 1);
+    for (int k = 0; k < per_graph; ++k) {
+      void* p = nullptr;
+      const cudaError_t e = mode == G500_DELIVER_DEVICE ? cudaMalloc(&p, bytes)
+                                                        : cudaHostAlloc(&p, bytes, cudaHostAllocDefault);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        free_delivery(s);
+        return g500::set_error(G500_E_NOMEM, "delivery buffers: %s", cudaGetErrorString(e));
+      }
+      s->slots[g].push_back(static_cast<uint8_t*>(p));
+      s->free_slots[g].push_back(k);
+    }
+  }
+  s->delivery = mode;
   return G500_OK;
 }

@@ -214,6 +214,22 @@ struct StaticScratch {
 static StaticScratch g_static_scratch[64];
 static std::mutex g_static_mu;
 
+// G500_OK when p is device (or managed) memory of device dev.
+static int on_device(const void* p, int dev, const char* what) {
+  cudaPointerAttributes a;
+  const cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(G500_E_INVAL, "%s: not a CUDA pointer (%s)", what, cudaGetErrorString(e));
+  }
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+    return set_error(G500_E_INVAL, "%s is not in device memory", what);
+  if (a.type == cudaMemoryTypeDevice && a.device != dev)
+    return set_error(G500_E_INVAL, "%s is on device %d, but device %d is current; make the device that holds the "
+                     "buffers current before the call", what, a.device, dev);
+  return G500_OK;
+}
+
 // Resolve this device's scratch addresses (first call on a device only).
 static int static_scratch(int dev, StaticScratch* out) {
   if (dev < 0 || dev >= 64) return set_error(G500_E_INVAL, "device %d out of range", dev);
@@ -245,6 +261,10 @@ extern "C" int g500_validate_noalloc(const g500_packed_edge* dev_edges, int64_t 
                      "use g500_validate", G500_VALIDATE_STATIC_MAX_VERTS, (long long)nlocalverts);
   int dev = 0;
   G500_CUDA(cudaGetDevice(&dev));
+  // the scratch and the kernels belong to the current device: pred and the
+  // edge list must live there too (a peer's or a host pointer is refused)
+  G500_TRY(on_device(dev_pred, dev, "pred"));
+  if (num_edges > 0) G500_TRY(on_device(dev_edges, dev, "edge list"));
   StaticScratch sc;
   G500_TRY(static_scratch(dev, &sc));
   cudaStream_t s = (cudaStream_t)stream;

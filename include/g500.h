@@ -338,7 +338,8 @@ typedef struct g500_server_config {
                                     (so that launches of other graphs run beside it); (0, 1] */
   int32_t plain_below;           /* a graph with at most this many waiting queries runs them one plain
                                     BFS each (0 never; negative: calibrated per graph at create) */
-  int32_t pad;
+  int32_t batch_target;          /* while a launch of a graph is in flight, another starts only once this
+                                    many of its queries wait (0, the default: whenever a worker is idle) */
 } g500_server_config;
 
 typedef struct g500_query_result {
@@ -374,7 +375,14 @@ typedef struct g500_serve_report {
   int64_t launches;
   int32_t max_in_flight;         /* launches running at once */
   int32_t workers;               /* launch slots created so far */
+  int32_t delivery;              /* G500_DELIVER_*: where each query's levels went before it completed */
+  int32_t pad;
 } g500_serve_report;
+
+/* Result delivery of the load generator's queries (g500_server_set_delivery). */
+#define G500_DELIVER_NONE 0   /* levels stay in the launch's workspace (completion only) */
+#define G500_DELIVER_DEVICE 1 /* each query's levels copied to a device buffer of its own */
+#define G500_DELIVER_HOST 2   /* each query's levels copied to a pinned host buffer of its own */
 
 int g500_server_default_config(g500_server_config* cfg);
 int g500_server_create(g500_graph* const* graphs, int num_graphs, const g500_server_config* cfg, g500_server** out);
@@ -390,10 +398,17 @@ int g500_server_info(g500_server* s, g500_server_info_t* info);
 /* Open-loop load: num_queries Poisson arrivals at rate_qps, each on a graph
  * chosen uniformly and a root chosen uniformly among vertices with at least
  * one edge (splitmix64 stream from seed); latency statistics skip the first
- * `warmup` queries. */
+ * `warmup` queries.  With a delivery mode set (g500_server_set_delivery) each
+ * query's level array (pred_size bytes) is copied to a buffer of its own
+ * before the query completes, so its latency includes delivering the result. */
 int g500_server_run_poisson(g500_server* s, double rate_qps, int64_t num_queries, uint64_t seed, int64_t warmup,
                             g500_serve_report* rep);
 int g500_server_destroy(g500_server* s);
+/* Where run_poisson delivers each query's levels: G500_DELIVER_NONE (default),
+ * _DEVICE or _HOST.  Waits for the queries in flight, then allocates per graph
+ * max_batch x max_workers_per_graph + 1 level buffers (a query waits for a free
+ * one); G500_E_NOMEM when they do not fit. */
+int g500_server_set_delivery(g500_server* s, int mode);
 
 /* Self-test of the failure path of the bounded grid barrier (no counterpart in
  * the reference): a cooperative launch in which one block never arrives must
@@ -415,7 +430,11 @@ int g500_selftest_barrier_timeout(int device, int* timed_out, int* recovered);
  * any stream capture.  Every call shares the same scratch: calls that overlap
  * on the GPU (e.g. on two streams) race and must be serialised by the caller.
  * stream may be NULL (the default stream); the call returns after the stream
- * has finished the validation. */
+ * has finished the validation.  The call runs on the device that is current
+ * when it is made: dev_pred and dev_edges must be that device's memory
+ * (otherwise G500_E_INVAL).  The scratch addresses are resolved once per device
+ * and kept for the life of the library: after a cudaDeviceReset the library
+ * must be unloaded and loaded again before this call is used on that device. */
 #define G500_VALIDATE_STATIC_MAX_VERTS (1 << 22)
 int g500_validate_noalloc(const g500_packed_edge* dev_edges, int64_t num_edges, int64_t nglobalverts,
                           int64_t nlocalverts, int64_t root, const int64_t* dev_pred, void* stream,

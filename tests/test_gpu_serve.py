@@ -66,8 +66,10 @@ def run_alone(g500, graphs, queries, **cfg):
     return out
 
 
-@pytest.mark.parametrize("plain_below", [-1, 0, 1000])  # calibrated, never plain, always plain
-def test_serve_levels_alone_and_in_mix(g500, served, plain_below):
+# plain_below: calibrated, never plain, always plain; batch_target 32: a second launch of a graph
+# waits until 32 of its queries wait (0, the default: no holding)
+@pytest.mark.parametrize("plain_below,batch_target", [(-1, 0), (0, 0), (1000, 0), (0, 32)])
+def test_serve_levels_alone_and_in_mix(g500, served, plain_below, batch_target):
     graphs, oracles, _ = served
     alone_q = pick_queries(graphs, 9, seed=1)
     alone = run_alone(g500, graphs, alone_q)
@@ -78,7 +80,8 @@ def test_serve_levels_alone_and_in_mix(g500, served, plain_below):
 
     # the mix: every alone query again, plus many more on every graph, submitted back to back
     mix_q = alone_q + pick_queries(graphs, 400, seed=2) + alone_q
-    srv = g500.Server(graphs, max_batch=128, max_workers_per_graph=2, plain_below=plain_below)
+    srv = g500.Server(graphs, max_batch=128, max_workers_per_graph=2, plain_below=plain_below,
+                      batch_target=batch_target)
     bufs, ids = [], []
     for gi, r in mix_q:
         b = np.full(graphs[gi].pred_size(), 7, np.uint8)
@@ -166,6 +169,23 @@ def test_serve_poisson_report(g500, served):
     assert rep["failed"] == 0 and rep["queries"] == 500
     assert 0 < rep["p50_ms"] <= rep["p99_ms"] <= rep["max_ms"]
     assert rep["gteps"] > 0 and rep["mean_batch"] >= 1 and rep["launches"] >= 1
+
+
+@pytest.mark.parametrize("mode", ["DELIVER_DEVICE", "DELIVER_HOST"])
+def test_serve_poisson_with_delivery(g500, served, mode):
+    """Each load-generator query's levels are copied to a buffer of its own before
+    it completes; the buffers are a bounded ring, so queries wait for a free one."""
+    graphs, _, _ = served
+    srv = g500.Server(graphs, max_batch=16, max_workers_per_graph=1)
+    srv.set_delivery(getattr(g500, mode))
+    rep = srv.run_poisson(20000.0, 600, seed=2026, warmup=100)
+    assert rep["failed"] == 0 and rep["queries"] == 500 and rep["delivery"] == getattr(g500, mode)
+    srv.set_delivery(g500.DELIVER_NONE)
+    rep2 = srv.run_poisson(20000.0, 300, seed=7)
+    assert rep2["failed"] == 0 and rep2["delivery"] == g500.DELIVER_NONE
+    with pytest.raises(g500.G500Error):
+        srv.set_delivery(7)
+    srv.close()
 
 
 def test_serve_rejects_bad_queries(g500, served):

@@ -75,3 +75,14 @@ def test_noalloc_refuses_sizes_beyond_its_scratch(g500):
     rc = L.g500_validate_noalloc(None, 0, 1, limit + 1, 0, pred.data_ptr(), None, C.byref(evc), C.byref(ok), None)
     assert rc == g500.G500_E_RANGE
     assert b"at most" in L.g500_last_error()
+
+
+def test_noalloc_refuses_buffers_off_the_current_device(g500):
+    """pred (or the edge list) that is not memory of the current device is refused
+    before any kernel runs; a host array stands in for another device's buffer."""
+    L = g500.lib()
+    host_pred = np.full(64, -1, dtype=np.int64)
+    evc, ok = C.c_int64(), C.c_int()
+    rc = L.g500_validate_noalloc(None, 0, 1, 64, 0, host_pred.ctypes.data, None, C.byref(evc), C.byref(ok), None)
+    assert rc == g500.G500_E_INVAL
+    assert b"device memory" in L.g500_last_error()
