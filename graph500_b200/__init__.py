@@ -28,6 +28,7 @@ LIB_PATH = os.path.join(HERE, "libg500.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "g500.h")
 USERSEED1, USERSEED2 = 2, 3  # mpi/parameters.h:190-191
 EDGE_DTYPE = np.dtype([("v0_low", "<u4"), ("v1_low", "<u4"), ("high", "<u4")])
+WEDGE_DTYPE = np.dtype([("v0_low", "<u4"), ("v1_low", "<u4"), ("high", "<u4"), ("weight", "<i4")])
 
 (G500_OK, G500_E_INVAL, G500_E_NOMEM, G500_E_DEVICE, G500_E_TIMEOUT, G500_E_RANGE, G500_E_STATE,
  G500_E_VALIDATION, G500_E_IO) = range(9)
@@ -146,6 +147,7 @@ def lib() -> C.CDLL:
         "g500_host_free": ([P], i32),
         "g500_scramble_values": ([i32, u64, u64, C.POINTER(u64), C.POINTER(u64)], i32),
         "g500_gen_edges": ([i32, i32, u64, u64, i64, i64, P, i32, P], i32),
+        "g500_gen_edges_spec2012": ([i32, i32, u64, u64, i64, i64, P, i32, P], i32),
         "g500_graph_build": ([P, i64, i32, i32, i32, i32, C.POINTER(P)], i32),
         "g500_graph_generate": ([i32, i32, u64, u64, i32, i32, C.POINTER(P)], i32),
         "g500_graph_info_get": ([P, C.POINTER(GraphInfo)], i32),
@@ -277,6 +279,23 @@ def generate_edges(scale: int, edgefactor: int = 16, start: int = 0, end: int | 
     if _nbytes(out) < (end - start) * EDGE_DTYPE.itemsize:
         raise ValueError("output buffer too small for the requested edge range")
     check(lib().g500_gen_edges(scale, edgefactor, seed1, seed2, start, end, ptr, int(dev), None))
+    return out
+
+
+def generate_edges_spec2012(scale: int, edgefactor: int = 16, start: int = 0, end: int | None = None,
+                            seed1: int = USERSEED1, seed2: int = USERSEED2, out=None):
+    """Weighted edges [start, end) of generate_graph_spec2012
+    (mpi/benchmark_helper.hpp:316-322), generated on the GPU: 2^scale - 1
+    binary-tree edges, then R-MAT edges (A = .55, B = C = .01); weight 0xBEEF."""
+    n = 1 << scale
+    if end is None:
+        end = n * edgefactor + n - 1
+    if out is None:
+        out = np.zeros(end - start, dtype=WEDGE_DTYPE)
+    ptr, dev = _ptr(out)
+    if _nbytes(out) < (end - start) * WEDGE_DTYPE.itemsize:
+        raise ValueError("output buffer too small for the requested edge range")
+    check(lib().g500_gen_edges_spec2012(scale, edgefactor, seed1, seed2, start, end, ptr, int(dev), None))
     return out
 
 

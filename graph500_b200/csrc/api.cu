@@ -34,17 +34,19 @@ extern "C" int g500_scramble_values(int scale, uint64_t s1, uint64_t s2, uint64_
   return G500_OK;
 }
 
-extern "C" int g500_gen_edges(int scale, int edgefactor, uint64_t s1, uint64_t s2, int64_t start, int64_t end,
-                              g500_packed_edge* out, int out_on_device, void* stream) {
-  if (scale < 1 || scale > 48) return set_error(G500_E_INVAL, "scale %d not in 1..48", scale);
-  if (edgefactor < 1) return set_error(G500_E_INVAL, "edgefactor %d < 1", edgefactor);
+namespace {
+// Edges [start, end) of a graph of `total` edges into out (device or host
+// memory); host output is generated on the device in chunks and copied back.
+template <typename Edge, typename Gen>
+int gen_edges_to(int scale, int64_t total, int64_t start, int64_t end, Edge* out, int out_on_device, void* stream,
+                 Gen gen) {
   if (start < 0 || end < start) return set_error(G500_E_INVAL, "bad edge range [%lld, %lld)", (long long)start,
                                                  (long long)end);
-  if (end > (int64_t(1) << scale) * edgefactor)
-    return set_error(G500_E_RANGE, "edge range ends past the graph's %lld edges",
-                     (long long)((int64_t(1) << scale) * edgefactor));
+  if (end > total)
+    return set_error(G500_E_RANGE, "edge range ends past the graph's %lld edges", (long long)total);
   if (!out && end > start) return set_error(G500_E_INVAL, "null output");
   if (end == start) return G500_OK;
+  (void)scale;
   cudaStream_t s = (cudaStream_t)stream;
   cudaStream_t own = nullptr;
   if (!s) {
@@ -53,7 +55,7 @@ extern "C" int g500_gen_edges(int scale, int edgefactor, uint64_t s1, uint64_t s
   }
   int st = G500_OK;
   if (out_on_device) {
-    st = gen_edges_device(scale, s1, s2, start, end, out, s);
+    st = gen(start, end, out, s);
     if (own) {
       cudaError_t e = cudaStreamSynchronize(own);
       if (st == G500_OK && e != cudaSuccess) st = cuda_error(e, "generation", __FILE__, __LINE__);
@@ -61,14 +63,13 @@ extern "C" int g500_gen_edges(int scale, int edgefactor, uint64_t s1, uint64_t s
   } else {
     // generate into device memory chunk by chunk and copy back
     const int64_t chunk = int64_t(1) << 26;
-    g500_packed_edge* d = nullptr;
+    Edge* d = nullptr;
     st = dev_alloc_n(&d, std::min<int64_t>(chunk, end - start), "generation staging");
     for (int64_t b = start; st == G500_OK && b < end; b += chunk) {
       int64_t e = std::min<int64_t>(end, b + chunk);
-      st = gen_edges_device(scale, s1, s2, b, e, d, s);
+      st = gen(b, e, d, s);
       if (st == G500_OK) {
-        cudaError_t ce = cudaMemcpyAsync(out + (b - start), d, sizeof(g500_packed_edge) * (e - b),
-                                         cudaMemcpyDeviceToHost, s);
+        cudaError_t ce = cudaMemcpyAsync(out + (b - start), d, sizeof(Edge) * (e - b), cudaMemcpyDeviceToHost, s);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
         if (ce != cudaSuccess) st = cuda_error(ce, "generation copy", __FILE__, __LINE__);
       }
@@ -77,4 +78,26 @@ extern "C" int g500_gen_edges(int scale, int edgefactor, uint64_t s1, uint64_t s
   }
   if (own) cudaStreamDestroy(own);
   return st;
+}
+}  // namespace
+
+extern "C" int g500_gen_edges(int scale, int edgefactor, uint64_t s1, uint64_t s2, int64_t start, int64_t end,
+                              g500_packed_edge* out, int out_on_device, void* stream) {
+  if (scale < 1 || scale > 48) return set_error(G500_E_INVAL, "scale %d not in 1..48", scale);
+  if (edgefactor < 1) return set_error(G500_E_INVAL, "edgefactor %d < 1", edgefactor);
+  return gen_edges_to(scale, (int64_t(1) << scale) * edgefactor, start, end, out, out_on_device, stream,
+                      [&](int64_t b, int64_t e, g500_packed_edge* o, cudaStream_t s) {
+                        return gen_edges_device(scale, s1, s2, b, e, o, s);
+                      });
+}
+
+extern "C" int g500_gen_edges_spec2012(int scale, int edgefactor, uint64_t s1, uint64_t s2, int64_t start,
+                                       int64_t end, g500_weighted_edge* out, int out_on_device, void* stream) {
+  if (scale < 1 || scale > 48) return set_error(G500_E_INVAL, "scale %d not in 1..48", scale);
+  if (edgefactor < 1) return set_error(G500_E_INVAL, "edgefactor %d < 1", edgefactor);
+  const int64_t n = int64_t(1) << scale;
+  return gen_edges_to(scale, n * edgefactor + n - 1, start, end, out, out_on_device, stream,
+                      [&](int64_t b, int64_t e, g500_weighted_edge* o, cudaStream_t s) {
+                        return gen_edges_spec2012_device(scale, s1, s2, b, e, o, s);
+                      });
 }

@@ -75,6 +75,8 @@ int radix_sort_u64(uint64_t* keys, uint64_t* alt, int64_t n, int lo_bit, int hi_
 struct GenPlan;  // defined in gen.cu
 int gen_edges_device(int scale, uint64_t seed1, uint64_t seed2, int64_t start, int64_t end,
                      g500_packed_edge* out, cudaStream_t s);
+int gen_edges_spec2012_device(int scale, uint64_t seed1, uint64_t seed2, int64_t start, int64_t end,
+                              g500_weighted_edge* out, cudaStream_t s);
 
 // 5x5 transition matrices mod 2^31-1 on the host
 struct Mat5 { uint32_t m[25]; };

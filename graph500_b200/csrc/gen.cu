@@ -122,6 +122,8 @@ struct GenParams {
   uint64_t val0, val1; // scramble words
   int scale;
   int64_t start, end;
+  uint32_t a_num, bc_num;  // R-MAT initiator numerators of 10000 (A; B = C)
+  int64_t n_init;          // initial edges before the R-MAT ones (binary tree: N - 1)
 };
 
 // Mersenne folding: x mod (2^31 - 1) without a division.
@@ -161,21 +163,46 @@ __device__ __forceinline__ uint64_t scramble_dev(uint64_t v, int scale, uint64_t
   return v;
 }
 
-// generate_4way_bernoulli, graph_generator.hpp:651-677 (no noise, A=.57, B=C=.19)
-__device__ __forceinline__ int bernoulli4_dev(uint32_t z[5]) {
+// generate_4way_bernoulli, graph_generator.hpp:651-677 (no noise): spec 2010
+// A = .57, B = C = .19 (numerators 5700 / 1900); spec 2012 A = .55, B = C = .01
+__device__ __forceinline__ int bernoulli4_dev(uint32_t z[5], uint32_t a_num, uint32_t bc_num) {
   uint32_t val = mrg_next_dev(z);
   while (val < 7295u) val = mrg_next_dev(z);  // 0xFFFFFFFF % 10000
   val %= 10000u;
-  if (val < 1900u) return 1;
-  val -= 1900u;
-  if (val < 1900u) return 2;
-  val -= 1900u;
-  if (val < 5700u) return 0;
+  if (val < bc_num) return 1;
+  val -= bc_num;
+  if (val < bc_num) return 2;
+  val -= bc_num;
+  if (val < a_num) return 0;
   return 3;
 }
 
+__device__ __forceinline__ void put_edge(g500_packed_edge* out, int64_t i, uint64_t v0, uint64_t v1) {
+  g500_packed_edge pe;
+  pe.v0_low = (uint32_t)v0;
+  pe.v1_low = (uint32_t)v1;
+  pe.high = (uint32_t)(((v0 >> 32) & 0xFFFF) | ((v1 >> 16) & 0xFFFF0000u));
+  out[i] = pe;
+}
+
+// WeightedEdge (primitives.hpp:87-106): the packed layout and a weight, which
+// generateWeight sets to the constant 0xBEEF (graph_generator.hpp:495-503)
+__device__ __forceinline__ void put_edge(g500_weighted_edge* out, int64_t i, uint64_t v0, uint64_t v1) {
+  g500_weighted_edge w;  // 4-byte aligned: a caller's buffer need not be 16-byte aligned
+  w.v0_low = (uint32_t)v0;
+  w.v1_low = (uint32_t)v1;
+  w.high = (uint32_t)(((v0 >> 32) & 0xFFFF) | ((v1 >> 16) & 0xFFFF0000u));
+  w.weight = 0xBEEF;
+  out[i] = w;
+}
+
+// Thread t of T owns edges start + t, start + t + T, ...: edges below n_init
+// are the binary-tree initial edges (scramble(i + 1), scramble((i + 1) / 2))
+// (generateInitialEdge, graph_generator.hpp:513-520), the others R-MAT edges
+// from the stream of their own index (generateRange, :612-627).
+template <typename Edge>
 __global__ void __launch_bounds__(256) gen_edges_kernel(GenParams p, const uint32_t* __restrict__ skip_mid,
-                                                        g500_packed_edge* __restrict__ out) {
+                                                        Edge* __restrict__ out) {
   __shared__ uint32_t step[25];
   if (threadIdx.x < 25) step[threadIdx.x] = p.step[threadIdx.x];
   __syncthreads();
@@ -191,23 +218,23 @@ __global__ void __launch_bounds__(256) gen_edges_kernel(GenParams p, const uint3
     if (v) mat5_apply_dev(skip_mid + ((size_t)b * 256 + v) * 25, z);
   }
   for (; ei < p.end; ei += T) {
-    uint32_t s[5] = {z[0], z[1], z[2], z[3], z[4]};
-    // make_one_edge, graph_generator.hpp:681-704
-    int64_t base_src = 0, base_tgt = 0;
-    for (int lvl = p.scale - 1; lvl >= 0; --lvl) {
-      int sq = bernoulli4_dev(s);
-      int so = sq >> 1, to = sq & 1;
-      if (base_src == base_tgt && so > to) { int x = so; so = to; to = x; }
-      base_src += (int64_t)so << lvl;
-      base_tgt += (int64_t)to << lvl;
+    if (ei < p.n_init) {
+      put_edge(out, ei - p.start, scramble_dev((uint64_t)(ei + 1), p.scale, p.val0, p.val1),
+               scramble_dev((uint64_t)((ei + 1) / 2), p.scale, p.val0, p.val1));
+    } else {
+      uint32_t s[5] = {z[0], z[1], z[2], z[3], z[4]};
+      // make_one_edge, graph_generator.hpp:681-704
+      int64_t base_src = 0, base_tgt = 0;
+      for (int lvl = p.scale - 1; lvl >= 0; --lvl) {
+        int sq = bernoulli4_dev(s, p.a_num, p.bc_num);
+        int so = sq >> 1, to = sq & 1;
+        if (base_src == base_tgt && so > to) { int x = so; so = to; to = x; }
+        base_src += (int64_t)so << lvl;
+        base_tgt += (int64_t)to << lvl;
+      }
+      put_edge(out, ei - p.start, scramble_dev((uint64_t)base_src, p.scale, p.val0, p.val1),
+               scramble_dev((uint64_t)base_tgt, p.scale, p.val0, p.val1));
     }
-    uint64_t v0 = scramble_dev((uint64_t)base_src, p.scale, p.val0, p.val1);
-    uint64_t v1 = scramble_dev((uint64_t)base_tgt, p.scale, p.val0, p.val1);
-    g500_packed_edge pe;
-    pe.v0_low = (uint32_t)v0;
-    pe.v1_low = (uint32_t)v1;
-    pe.high = (uint32_t)(((v0 >> 32) & 0xFFFF) | ((v1 >> 16) & 0xFFFF0000u));
-    out[ei - p.start] = pe;
     mat5_apply_dev(step, z);
   }
 }
@@ -239,8 +266,9 @@ static int skip_mid_table(uint32_t** out) {
   return G500_OK;
 }
 
-int gen_edges_device(int scale, uint64_t s1, uint64_t s2, int64_t start, int64_t end,
-                     g500_packed_edge* out, cudaStream_t s) {
+template <typename Edge>
+static int gen_device(int scale, uint64_t s1, uint64_t s2, int64_t start, int64_t end, uint32_t a_num,
+                      uint32_t bc_num, int64_t n_init, Edge* out, cudaStream_t s) {
   if (end <= start) return G500_OK;
   uint32_t* skip_mid = nullptr;
   G500_TRY(skip_mid_table(&skip_mid));
@@ -268,9 +296,25 @@ int gen_edges_device(int scale, uint64_t s1, uint64_t s2, int64_t start, int64_t
   p.scale = scale;
   p.start = start;
   p.end = end;
-  gen_edges_kernel<<<(unsigned)blocks, threads, 0, s>>>(p, skip_mid, out);
+  p.a_num = a_num;
+  p.bc_num = bc_num;
+  p.n_init = n_init;
+  gen_edges_kernel<Edge><<<(unsigned)blocks, threads, 0, s>>>(p, skip_mid, out);
   G500_CUDA(cudaGetLastError());
   return G500_OK;
+}
+
+// generate_graph_spec2010 (benchmark_helper.hpp:308-314)
+int gen_edges_device(int scale, uint64_t s1, uint64_t s2, int64_t start, int64_t end,
+                     g500_packed_edge* out, cudaStream_t s) {
+  return gen_device(scale, s1, s2, start, end, 5700u, 1900u, 0, out, s);
+}
+
+// generate_graph_spec2012 (benchmark_helper.hpp:316-322): RmatGraphGenerator<
+// WeightedEdge, 5500, 100> with InitialEdgeType::BINARY_TREE (N - 1 initial edges)
+int gen_edges_spec2012_device(int scale, uint64_t s1, uint64_t s2, int64_t start, int64_t end,
+                              g500_weighted_edge* out, cudaStream_t s) {
+  return gen_device(scale, s1, s2, start, end, 5500u, 100u, (int64_t(1) << scale) - 1, out, s);
 }
 
 }  // namespace g500

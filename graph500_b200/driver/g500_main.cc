@@ -4,6 +4,10 @@
 //
 //   g500_main SCALE [EDGEFACTOR] [--roots N] [--reorder 0|1|2] [--max-runs K]
 //             [--pre-exec SECONDS] [--autotune]
+//   g500_main --print-result LOGFILE_PATH
+//
+// --print-result prints the result block of the runs a resume file holds,
+// without a GPU (the statistics of print_bfs_result, logfile.h:49-107).
 //
 // LOGFILE=path resumes an interrupted run as the reference does
 // (benchmark_helper.hpp:530-604): the file keeps SCALE, edgefactor, the
@@ -129,7 +133,33 @@ void print_result(int scale, int edgefactor, int nroots, double gen, double cons
 void usage() {
   std::fprintf(stderr,
                "usage: g500_main SCALE [EDGEFACTOR] [--roots N] [--reorder 0|1|2] [--max-runs K] "
-               "[--pre-exec SECONDS] [--autotune]\n");
+               "[--pre-exec SECONDS] [--autotune]\n"
+               "       g500_main --print-result LOGFILE_PATH\n");
+}
+
+// The result block of the finished runs of a resume file.
+int print_log_result(const char* path) {
+  LogFileFormat log;
+  FILE* fp = std::fopen(path, "rb");
+  if (!fp) {
+    std::fprintf(stderr, "cannot open %s\n", path);
+    return 1;
+  }
+  const size_t got = std::fread(&log, sizeof(log), 1, fp);
+  std::fclose(fp);
+  if (got != 1 || log.num_runs < 1 || log.num_runs > 64) {
+    std::fprintf(stderr, "%s is not a log file with finished runs\n", path);
+    return 1;
+  }
+  std::vector<double> bfs, val, edges;
+  for (int i = 0; i < log.num_runs; ++i) {
+    bfs.push_back(log.times[i].bfs_time);
+    val.push_back(log.times[i].validate_time);
+    edges.push_back((double)log.times[i].edge_counts);
+  }
+  print_result(log.scale, log.edge_factor, log.num_runs, log.generation_time, log.construction_time, bfs, val, edges,
+               true);
+  return 0;
 }
 
 }  // namespace
@@ -143,6 +173,8 @@ int main(int argc, char** argv) {
     if (a == "--help" || a == "-h") {
       usage();
       return 0;
+    } else if (a == "--print-result" && i + 1 < argc) {
+      return print_log_result(argv[i + 1]);
     } else if (a == "--roots" && i + 1 < argc) {
       nroots = std::atoi(argv[++i]);
     } else if (a == "--reorder" && i + 1 < argc) {

@@ -84,6 +84,28 @@ int g500_gen_edges(int scale, int edgefactor, uint64_t userseed1, uint64_t users
                    int64_t start, int64_t end, g500_packed_edge* out, int out_on_device,
                    void* stream);
 
+/* WeightedEdge (mpi/primitives.hpp:87-106): the packed edge and an int weight. */
+typedef struct g500_weighted_edge {
+  uint32_t v0_low;
+  uint32_t v1_low;
+  uint32_t high;
+  int32_t weight;
+} g500_weighted_edge;
+
+/* Edges [start, end) of the spec-2012 graph, bit-exact to
+ * generate_graph_spec2012 (benchmark_helper.hpp:316-322):
+ * RmatGraphGenerator<WeightedEdge, 5500, 100> (A = .55, B = C = .01) with
+ * InitialEdgeType::BINARY_TREE, i.e. 2^scale * edgefactor + 2^scale - 1 edges,
+ * of which edge i < 2^scale - 1 is (scramble(i + 1), scramble((i + 1) / 2))
+ * (graph_generator.hpp:385-392, :513-520) and every later edge the R-MAT edge
+ * of its index's stream (:612-627).  The weight is the reference's constant
+ * 0xBEEF (generateWeight, :495-503, whose random draw is disabled); its SSSP
+ * (run_sssp, bfs.hpp:2569-2571) is an empty stub, so nothing consumes the
+ * weights.  out, out_on_device, stream as for g500_gen_edges. */
+int g500_gen_edges_spec2012(int scale, int edgefactor, uint64_t userseed1, uint64_t userseed2,
+                            int64_t start, int64_t end, g500_weighted_edge* out, int out_on_device,
+                            void* stream);
+
 /* ---------------------------------------------------- (b) construction */
 /* BfsBase::construct(EdgeList*) (mpi/bfs.hpp:102-113 ->
  * GraphConstructor2DCSR::construct, graph_constructor.hpp:554-574).

@@ -16,6 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 USERSEED1, USERSEED2 = 2, 3  # mpi/parameters.h:190-191
 EDGE_DTYPE = np.dtype([("v0_low", "<u4"), ("v1_low", "<u4"), ("high", "<u4")])
+WEDGE_DTYPE = np.dtype([("v0_low", "<u4"), ("v1_low", "<u4"), ("high", "<u4"), ("weight", "<i4")])
 
 INFO_NAMES = ("log_orig_global_verts", "pred_size", "num_local_verts",
               "num_global_verts", "num_global_edges", "max_used_vertex")
@@ -42,6 +43,7 @@ def lib() -> C.CDLL:
         P = C.c_void_p
         i64, u64, i32 = C.c_int64, C.c_uint64, C.c_int
         L.orc_generate_edges.argtypes = [i32, i32, u64, u64, i64, i64, P]
+        L.orc_generate_edges_spec2012.argtypes = [i32, i32, u64, u64, i64, i64, P]
         L.orc_scramble_values.argtypes = [i32, u64, u64, P, P]
         L.orc_make_random_numbers.argtypes = [i64, u64, u64, i64, P]
         L.orc_mrg_skip_matrix.argtypes = [i32, i32, P]
@@ -77,6 +79,19 @@ def generate_edges(scale: int, edgefactor: int = 16, start: int = 0, end: int | 
         end = (1 << scale) * edgefactor
     out = np.zeros(end - start, dtype=EDGE_DTYPE)
     lib().orc_generate_edges(scale, edgefactor, seed1, seed2, start, end, _p(out))
+    return out
+
+
+def generate_edges_spec2012(scale: int, edgefactor: int = 16, start: int = 0, end: int | None = None,
+                            seed1: int = USERSEED1, seed2: int = USERSEED2) -> np.ndarray:
+    """Weighted edges [start, end) of generate_graph_spec2012
+    (mpi/benchmark_helper.hpp:316-322): N - 1 binary-tree edges, then R-MAT
+    edges with A = .55, B = C = .01; weight 0xBEEF."""
+    n = 1 << scale
+    if end is None:
+        end = n * edgefactor + n - 1
+    out = np.zeros(end - start, dtype=WEDGE_DTYPE)
+    lib().orc_generate_edges_spec2012(scale, edgefactor, seed1, seed2, start, end, _p(out))
     return out
 
 
@@ -218,6 +233,18 @@ class Reference:
     def generate(self, scale: int, edgefactor: int = 16) -> float:
         self.scale, self.edgefactor = scale, edgefactor
         return self.L.ref_generate(scale, edgefactor)
+
+    def generate_spec2012(self, scale: int, edgefactor: int = 16) -> np.ndarray:
+        """The reference's generate_graph_spec2012 edge list (weighted, 16 bytes per edge)."""
+        L = self.L
+        L.ref_generate_spec2012.argtypes = [C.c_int, C.c_int]
+        L.ref_generate_spec2012.restype = C.c_int64
+        L.ref_copy_edges_spec2012.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
+        L.ref_copy_edges_spec2012.restype = C.c_int64
+        n = L.ref_generate_spec2012(scale, edgefactor)
+        out = np.zeros(n, WEDGE_DTYPE)
+        got = L.ref_copy_edges_spec2012(_p(out), 0, n)
+        return out[:got]
 
     def edges(self, start: int = 0, count: int | None = None) -> np.ndarray:
         if count is None:

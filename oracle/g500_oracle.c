@@ -193,19 +193,39 @@ int64_t orc_scramble(int64_t v0, int scale, uint64_t val0, uint64_t val1) {
   return (int64_t)v;
 }
 
-/* graph_generator.hpp:651-677 with SPK_NOISE_LEVEL 0 and the spec-2010
- * initiator numerators A=5700, B=C=1900 of 10000 (benchmark_helper.hpp:311). */
-static inline int bernoulli4(orc_mrg_state* st) {
+/* graph_generator.hpp:651-677 with SPK_NOISE_LEVEL 0; initiator numerators
+ * of 10000: spec 2010 A=5700, B=C=1900 (benchmark_helper.hpp:311), spec 2012
+ * A=5500, B=C=100 (benchmark_helper.hpp:319). */
+static inline int bernoulli4(orc_mrg_state* st, uint32_t a_num, uint32_t bc_num) {
   const uint32_t limit = 0xFFFFFFFFu % 10000u; /* 7295 */
   uint32_t val = orc_mrg_get_uint_orig(st);
   while (val < limit) val = orc_mrg_get_uint_orig(st);
   val %= 10000u;
-  if (val < 1900u) return 1;
-  val -= 1900u;
-  if (val < 1900u) return 2;
-  val -= 1900u;
-  if (val < 5700u) return 0;
+  if (val < bc_num) return 1;
+  val -= bc_num;
+  if (val < bc_num) return 2;
+  val -= bc_num;
+  if (val < a_num) return 0;
   return 3;
+}
+
+/* make_one_edge (graph_generator.hpp:681-704): R-MAT descent with
+ * clip-and-flip from the stream of edge ei (ei * 2^64, :622-625). */
+static void rmat_edge(const orc_mrg_state* seed, int scale, uint64_t val0, uint64_t val1, int64_t ei,
+                      uint32_t a_num, uint32_t bc_num, int64_t* src, int64_t* tgt) {
+  orc_mrg_state st = *seed;
+  orc_mrg_skip(&st, 0, (uint64_t)ei, 0);
+  int64_t nverts = INT64_C(1) << scale, base_src = 0, base_tgt = 0;
+  while (nverts > 1) {
+    int square = bernoulli4(&st, a_num, bc_num);
+    int src_off = square / 2, tgt_off = square % 2;
+    if (base_src == base_tgt && src_off > tgt_off) { int t = src_off; src_off = tgt_off; tgt_off = t; }
+    nverts /= 2;
+    base_src += nverts * src_off;
+    base_tgt += nverts * tgt_off;
+  }
+  *src = orc_scramble(base_src, scale, val0, val1);
+  *tgt = orc_scramble(base_tgt, scale, val0, val1);
 }
 
 void orc_generate_edges(int scale, int edgefactor, uint64_t s1, uint64_t s2,
@@ -216,24 +236,44 @@ void orc_generate_edges(int scale, int edgefactor, uint64_t s1, uint64_t s2,
   orc_make_mrg_seed(s1, s2, &seed);
   uint64_t val0, val1;
   orc_scramble_values(scale, s1, s2, &val0, &val1);
-  const int64_t nverts0 = INT64_C(1) << scale;
 #pragma omp parallel for schedule(static)
   for (int64_t ei = start; ei < end; ++ei) {
-    /* graph_generator.hpp:622-625: each edge owns the stream at ei * 2^64. */
-    orc_mrg_state st = seed;
-    orc_mrg_skip(&st, 0, (uint64_t)ei, 0);
-    /* graph_generator.hpp:681-704: R-MAT descent with clip-and-flip. */
-    int64_t nverts = nverts0, base_src = 0, base_tgt = 0;
-    while (nverts > 1) {
-      int square = bernoulli4(&st);
-      int src_off = square / 2, tgt_off = square % 2;
-      if (base_src == base_tgt && src_off > tgt_off) { int t = src_off; src_off = tgt_off; tgt_off = t; }
-      nverts /= 2;
-      base_src += nverts * src_off;
-      base_tgt += nverts * tgt_off;
+    int64_t a, b;
+    rmat_edge(&seed, scale, val0, val1, ei, 5700u, 1900u, &a, &b);
+    edge_set(&out[ei - start], a, b);
+  }
+}
+
+/* generate_graph_spec2012 (benchmark_helper.hpp:316-322):
+ * RmatGraphGenerator<WeightedEdge, 5500, 100> with BINARY_TREE initial edges.
+ * Edge i < N - 1 is (scramble(i + 1), scramble((i + 1) / 2))
+ * (graph_generator.hpp:385-392, :513-520); later edges are R-MAT edges of
+ * their own index (:612-627); every weight is 0xBEEF (generateWeight,
+ * :495-503, the random draw disabled). */
+void orc_generate_edges_spec2012(int scale, int edgefactor, uint64_t s1, uint64_t s2,
+                                 int64_t start, int64_t end, orc_weighted_edge* out) {
+  (void)edgefactor;
+  build_skip_table();
+  orc_mrg_state seed;
+  orc_make_mrg_seed(s1, s2, &seed);
+  uint64_t val0, val1;
+  orc_scramble_values(scale, s1, s2, &val0, &val1);
+  const int64_t n_init = (INT64_C(1) << scale) - 1;
+#pragma omp parallel for schedule(static)
+  for (int64_t ei = start; ei < end; ++ei) {
+    int64_t a, b;
+    if (ei < n_init) {
+      a = orc_scramble(ei + 1, scale, val0, val1);
+      b = orc_scramble((ei + 1) / 2, scale, val0, val1);
+    } else {
+      rmat_edge(&seed, scale, val0, val1, ei, 5500u, 100u, &a, &b);
     }
-    edge_set(&out[ei - start], orc_scramble(base_src, scale, val0, val1),
-             orc_scramble(base_tgt, scale, val0, val1));
+    orc_packed_edge pe;
+    edge_set(&pe, a, b);
+    out[ei - start].v0_low = pe.v0_low;
+    out[ei - start].v1_low = pe.v1_low;
+    out[ei - start].high = pe.high;
+    out[ei - start].weight = 0xBEEF;
   }
 }
 

@@ -45,6 +45,10 @@ int64_t  orc_scramble(int64_t v, int scale, uint64_t val0, uint64_t val1);
  * to out[0 .. end-start).  OpenMP parallel over edge indices. */
 void     orc_generate_edges(int scale, int edgefactor, uint64_t userseed1, uint64_t userseed2,
                             int64_t start, int64_t end, orc_packed_edge* out);
+/* WeightedEdge, mpi/primitives.hpp:87-106 */
+typedef struct orc_weighted_edge { uint32_t v0_low, v1_low, high; int32_t weight; } orc_weighted_edge;
+void     orc_generate_edges_spec2012(int scale, int edgefactor, uint64_t userseed1, uint64_t userseed2,
+                                     int64_t start, int64_t end, orc_weighted_edge* out);
 
 /* ---- graph construction (mpi/graph_constructor.hpp, one rank) ---- */
 typedef struct orc_graph orc_graph;

@@ -137,7 +137,62 @@ REF_API int ref_validate(int64_t root, int64_t* pred, int64_t* edge_visit_count)
 
 REF_API void ref_end_bfs() { g_bfs->end_bfs(); }
 
+/* The reference's print_bfs_result (logfile.h:49-107) on given runs, to stdout. */
+REF_API void ref_print_bfs_result(int n, double* bfs_times, double* validate_times, double* edge_counts, int ok) {
+  print_bfs_result(n, bfs_times, validate_times, edge_counts, ok != 0);
+  fflush(stdout);
+}
+
+/* generate_graph_spec2012 (benchmark_helper.hpp:316-322) into a weighted edge
+ * list of its own (main.cc never calls it; the generator is compiled from the
+ * reference as it stands).  max_weight is unused by the reference's constant
+ * weight.  Returns the number of edges. */
+typedef EdgeListStorage<WeightedEdge, 8 * 1024 * 1024> RefWeightedEdgeList;
+static RefWeightedEdgeList* g_wedges = NULL;
+
+REF_API int64_t ref_generate_spec2012(int scale, int edgefactor) {
+  if (!g_setup) {
+    static char arg0[] = "ref_driver";
+    static char* argv[] = {arg0, NULL};
+    setup_globals(1, argv, scale, edgefactor);
+    g_setup = true;
+  }
+  delete g_wedges;
+  const int64_t n = int64_t(1) << scale;
+  g_wedges = new RefWeightedEdgeList(n * edgefactor + n, NULL);
+  generate_graph_spec2012(g_wedges, scale, edgefactor, 255);
+  int loops = g_wedges->beginRead(false);
+  int64_t total = 0;
+  for (int l = 0; l < loops; ++l) {
+    WeightedEdge* buf;
+    total += g_wedges->read(&buf);
+  }
+  g_wedges->endRead();
+  return total;
+}
+
+/* Copies weighted edges [start, start+count) into out (16 bytes each). */
+REF_API int64_t ref_copy_edges_spec2012(void* out, int64_t start, int64_t count) {
+  if (!g_wedges) return -1;
+  int loops = g_wedges->beginRead(false);
+  int64_t pos = 0, copied = 0;
+  for (int l = 0; l < loops; ++l) {
+    WeightedEdge* buf;
+    int n = g_wedges->read(&buf);
+    int64_t lo = std::max<int64_t>(start, pos), hi = std::min<int64_t>(start + count, pos + n);
+    if (hi > lo) {
+      memcpy((char*)out + (lo - start) * sizeof(WeightedEdge), buf + (lo - pos),
+             (size_t)(hi - lo) * sizeof(WeightedEdge));
+      copied += hi - lo;
+    }
+    pos += n;
+  }
+  g_wedges->endRead();
+  return copied;
+}
+
 REF_API void ref_release() {
+  delete g_wedges; g_wedges = NULL;
   delete g_bfs; g_bfs = NULL;
   delete g_edges; g_edges = NULL;
 }

@@ -88,11 +88,47 @@ def one_case(scale: int, vr: int, nroots: int) -> None:
     print("wrote", name, file=sys.stderr)
 
 
+# spec-2012 generator fixtures (generate_graph_spec2012, benchmark_helper.hpp:316-322)
+SPEC2012_SCALES = [4, 10, 12, 16]
+
+
+def spec2012_case(scale: int) -> None:
+    import oracle as O
+    ref = O.Reference(0)
+    e = ref.generate_spec2012(scale, 16)
+    # the digest covers the endpoints (the first 12 bytes of each 16-byte
+    # WeightedEdge).  The reference's weights are racy: generateWeight's
+    # per-thread loop (graph_generator.hpp:488-503) has no barrier before the
+    # master thread copies the chunk out (benchmark_helper.hpp:270-284, the
+    # barrier is compiled for the Intel compiler only), so a weight is 0xBEEF or
+    # whatever the chunk buffer held; the count of 0xBEEF weights is recorded
+    ends = np.ascontiguousarray(e.view(np.uint32).reshape(-1, 4)[:, :3])
+    rec = {"scale": scale, "edgefactor": 16, "num_edges": len(e), "endpoints_sha256": digest(ends),
+           "weights_0xBEEF": int((e["weight"] == 0xBEEF).sum())}
+    name = f"ref_spec2012_s{scale}"
+    with open(os.path.join(HERE, name + ".json"), "w") as f:
+        json.dump(rec, f, indent=1)
+    n = 1 << scale
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), edges_head=e[:64], edges_tail=e[-64:],
+                        edges_tree_end=e[n - 33:n + 31])
+    print("wrote", name, file=sys.stderr)
+
+
 def main() -> None:
     """No arguments: the small cases.  ``--large``: the benchmark sizes (minutes
-    of reference construction and validation each).  ``SCALE VR NROOTS``: one case."""
+    of reference construction and validation each).  ``--spec2012``: the
+    spec-2012 generator's edge lists.  ``SCALE VR NROOTS``: one case."""
     if len(sys.argv) == 4:
         one_case(int(sys.argv[1]), int(sys.argv[2]), int(sys.argv[3]))
+        return
+    if sys.argv[1:2] == ["--spec2012"]:
+        if len(sys.argv) == 3:
+            spec2012_case(int(sys.argv[2]))
+            return
+        for scale in SPEC2012_SCALES:
+            subprocess.run([sys.executable, __file__, "--spec2012", str(scale)], check=True,
+                           env=dict(os.environ, NO_AFFINITY="1"), stdout=subprocess.DEVNULL,
+                           stderr=subprocess.DEVNULL)
         return
     if sys.argv[1:] == ["--large"]:
         env = dict(os.environ, NO_AFFINITY="1")
