@@ -432,6 +432,45 @@ int g500_server_destroy(g500_server* s);
  * one); G500_E_NOMEM when they do not fit. */
 int g500_server_set_delivery(g500_server* s, int mode);
 
+/* ------------------------------------------- partitioned single-root BFS */
+/* One rank's share of a 1-D vertex partition for a BFS over several GPUs (or
+ * ranks emulated in one process).  The reference runs one root over a 2-D
+ * partition of MPI ranks, exchanging top-down "fold" packets to the owners of
+ * discovered vertices (mpi/bfs.hpp:521-572, :962-1137) and the bottom-up
+ * visited bitmap (bottom_up_comm.hpp:172-280) every level.  Here rank r of n
+ * owns the reordered vertex ids [32*S*r, 32*S*(r+1)) (S bitmap words each;
+ * g500_part_info) and the rows of those vertices in its replica of the CSR.
+ * The caller runs the level loop and the collectives (graph500_b200.partitioned
+ * does, over torch.distributed): per level every rank runs either
+ * g500_part_top_down (then an all-to-all of the (target << 32 | parent) pairs
+ * of g500_part_send_buffer, split by send_counts, and g500_part_apply of what
+ * it received) or g500_part_bottom_up, sums the level counters
+ * out[0..3] = {found, their degree sum, next frontier length, scanned} over the
+ * ranks, calls g500_part_compact before a top-down level that follows a
+ * bottom-up one, and all-gathers every rank's own slice (S words) into the
+ * full bitmap (nranks * S words) of every rank (g500_part_buffers; the
+ * slices and the bitmap are device memory, ordered on the rank's stream,
+ * which every call has finished when it returns).  g500_part_write_pred then
+ * writes pred (nolv entries, device memory) with this rank's reached vertices
+ * and -1 elsewhere; the element-wise max over the ranks is the run's pred
+ * (bfs.hpp:2651-2940 semantics: parent | level << 48, root = root).
+ * g500_part_begin out[0..2] = {root has edges, frontier length, frontier
+ * degree sum}.  A root without edges reached only itself: no rank lists it,
+ * the caller writes pred[root] = root. */
+#define G500_PART_MAX_RANKS 64
+typedef struct g500_part g500_part;
+int g500_part_create(g500_graph* g, int rank, int nranks, g500_part** out);
+int g500_part_info(const g500_part* p, int64_t* words_per_rank, int64_t* first_vertex, int64_t* end_vertex);
+int g500_part_buffers(g500_part* p, uint32_t** vis_full, uint32_t** own_slice, void** stream);
+int g500_part_begin(g500_part* p, int64_t root, int64_t* out);
+int g500_part_top_down(g500_part* p, int64_t frontier_edges, int64_t* send_counts);
+int g500_part_send_buffer(g500_part* p, uint64_t** pairs);
+int g500_part_apply(g500_part* p, const uint64_t* recv_pairs, int64_t num_pairs, int64_t* out);
+int g500_part_bottom_up(g500_part* p, int64_t* out);
+int g500_part_compact(g500_part* p, int64_t* num_frontier);
+int g500_part_write_pred(g500_part* p, int64_t* dev_pred);
+int g500_part_destroy(g500_part* p);
+
 /* Self-test of the failure path of the bounded grid barrier (no counterpart in
  * the reference): a cooperative launch in which one block never arrives must
  * end with the others giving up (*timed_out = 1) and leave the context usable

@@ -84,5 +84,5 @@ def test_spec2012_graph_builds_and_traverses(g500, oracle_mod):
         bfs.run_bfs(int(r), pred)
         lv = g500.levels_from_pred(pred)
         assert np.array_equal(lv, og.bfs_levels(int(r)))
-        assert (lv != 0xFFFF).all()
+        assert (lv[:1 << 12] != 0xFFFF).all()  # ids past 2^SCALE only pad pred_size
     bfs.close()
