@@ -53,10 +53,13 @@ constexpr uint64_t BFS_DEFERRED_PRED_BYTES = 100ull << 20;
 // level above it, in 32 bits instead of 64.  At SCALE 26 that halves the
 // array the final pass gathers from (131 MB against 262 MB), so most of the
 // gathers hit L2.  Graphs with more than 2^PACK_SHIFT vertex ids use 64-bit
-// entries; a search that reaches level PACK_LEVELS stops, and the host runs
-// it again with 64-bit entries (and keeps them for that handle).
+// entries; a search that reaches level PACK_LEVELS - 1 stops, and the host
+// runs it again with 64-bit entries (and keeps them for that handle), so that
+// the all-ones word never is an entry: it marks an unreached vertex
+// (PACK_NONE; -1 in 64-bit entries).
 constexpr int PACK_SHIFT = 27;
 constexpr int PACK_LEVELS = 1 << (32 - PACK_SHIFT);
+constexpr uint32_t PACK_NONE = 0xFFFFFFFFu;
 constexpr int BFS_MIN_BLOCKS = 2;        // co-resident blocks per SM (64 registers, no spills)
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
 constexpr int BU_WORDS = 4;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
@@ -102,15 +105,6 @@ template <int DEF>
 __device__ __forceinline__ void put_deferred(const RunParams& p, int64_t r, uint32_t parent, int64_t lvl) {
   if constexpr (DEF == 2) p.pred_p[r] = parent | ((uint32_t)(lvl >> 48) << PACK_SHIFT);
   else p.pred_r[r] = (int64_t)parent | lvl;
-}
-
-template <int DEF>
-__device__ __forceinline__ int64_t get_deferred(const RunParams& p, int64_t r) {
-  if constexpr (DEF == 2) {
-    const uint32_t e = __ldcg(p.pred_p + r);
-    return (int64_t)(e & ((1u << PACK_SHIFT) - 1u)) | ((int64_t)(e >> PACK_SHIFT) << 48);
-  }
-  return __ldcg(p.pred_r + r);
 }
 
 __device__ __forceinline__ uint32_t chunks_of(uint64_t deg) { return (uint32_t)((deg + TD_CHUNK - 1) / TD_CHUNK); }
@@ -554,8 +548,15 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   const uint64_t root_b = has_edges ? p.off[root_r] : 0;
   const uint64_t root_deg = has_edges ? p.off[root_r + 1] - root_b : 0;
   const int64_t root_items = (int64_t)chunks_of(root_deg);
-  if (DEF == 0 || !has_edges)  // deferred mode writes pred whole at the end
-    for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = i == p.root ? p.root : -1;
+  if (DEF == 0 || !has_edges) {  // deferred mode writes pred whole at the end
+    if (!(reinterpret_cast<uintptr_t>(p.pred) & 15)) {  // 16-byte stores (nolv is even)
+      longlong2* pv = reinterpret_cast<longlong2*>(p.pred);
+      for (int64_t i = tid; i < p.nolv / 2; i += nthreads)
+        pv[i] = make_longlong2(2 * i == p.root ? p.root : -1, 2 * i + 1 == p.root ? p.root : -1);
+    } else {
+      for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = i == p.root ? p.root : -1;
+    }
+  }
   if constexpr (DEF != 0)
     if (has_edges && tid == 0) put_deferred<DEF>(p, root_r, (uint32_t)p.root, 0);
   for (int64_t i = tid; i < p.nwords; i += nthreads)
@@ -599,7 +600,7 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   (blockIdx.x == 0 && threadIdx.x < P_NUM ? (void)(ctl->pos[(phase + 1) % 3][threadIdx.x] = 0) : (void)0), \
       ctl->cnt[phase % 3]
   for (;; ++level) {
-    if (DEF == 2 && level >= PACK_LEVELS) {  // the packed level field is full: the host reruns unpacked
+    if (DEF == 2 && level >= PACK_LEVELS - 1) {  // the packed level field is full: the host reruns unpacked
       if (tid == 0) atomicOr(&ctl->bar.err, (unsigned)BFS_ERR_PACK);
       return;
     }
@@ -676,6 +677,23 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
                    edges + (was_forward ? carried_in : 0), sect + (was_forward ? carried_in : 0), t_mid);
   }
 #undef NEXT_PHASE_SLOT
+  // deferred modes: the entries of the vertices the search did not reach (and
+  // of those without edges) become "unreached", so that the final pass reads
+  // one entry per vertex and no bitmap.  The last level's barrier has passed:
+  // the visited map is final.  Under VERTEX_REORDERING 2 few such vertices lie
+  // below nlv (those without edges sort last).
+  if constexpr (DEF != 0) {
+    const uint32_t* vf = p.vis[cur_vis];
+    for (int64_t wi = tid; wi < p.nwords; wi += nthreads) {
+      uint32_t miss = ~(__ldcg(vf + wi) & ~__ldg(p.vis_init + wi));
+      while (miss) {
+        const int b = __ffs(miss) - 1;
+        miss &= miss - 1;
+        if constexpr (DEF == 2) p.pred_p[wi * 32 + b] = PACK_NONE;
+        else p.pred_r[wi * 32 + b] = -1;
+      }
+    }
+  }
   if (tid == 0) {
     ctl->num_levels = (unsigned)level;
     ctl->final_vis = cur_vis;
@@ -684,44 +702,42 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
 }
 
 // Deferred modes, after the search: pred in original-id order with
-// sequential writes.  A reached vertex (visited now, not pre-visited for lack
-// of edges) takes its entry from pred_r.  Its own launch, so that 2048 threads
-// per SM (the persistent kernel has 1024) keep the gathers in flight; 4
-// consecutive vertices per thread, every load of a thread issued together
-// (an unreached vertex's entry is stale and dropped).  The streamed map and
-// pred are evict-first, so that the gathered bitmaps and entries stay in L2.
-// nolv is a multiple of 65536.
+// sequential writes.  The entry of reordered vertex r (r < nlv) is its pred
+// value, or "unreached" (PACK_NONE / -1, written by the search's last phase);
+// a vertex beyond nlv has no edges and no entry.  Its own launch, so that 2048
+// threads per SM (the persistent kernel has 1024) keep the gathers in flight;
+// 4 consecutive vertices per thread, their loads issued together.  The
+// streamed map and pred are evict-first, so that the gathered entries stay in
+// L2.  nolv is a multiple of 65536.
 constexpr int FINAL_THREADS = 256;
+template <int DEF>
+__device__ __forceinline__ long long final_entry(const RunParams& p, uint32_t r) {
+  if ((int64_t)r >= p.nlv) return -1ll;
+  if constexpr (DEF == 2) {
+    const uint32_t e = __ldcg(p.pred_p + r);
+    return e == PACK_NONE ? -1ll
+                          : (long long)((int64_t)(e & ((1u << PACK_SHIFT) - 1u)) | ((int64_t)(e >> PACK_SHIFT) << 48));
+  }
+  return (long long)__ldcg(p.pred_r + r);
+}
+
 template <int DEF>
 __global__ void __launch_bounds__(FINAL_THREADS, 8) deferred_pred_kernel(RunParams p) {
   const BfsCtl* ctl = p.ctl;
   if (!ctl->root_has_edges || ctl->bar.err) return;  // pred already written, or the search failed
-  const uint32_t* vf = p.vis[ctl->final_vis];
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
   if (reinterpret_cast<uintptr_t>(p.pred) & 15) {  // a caller's pred not 16-byte aligned: one entry at a time
-    for (int64_t u = tid; u < p.nolv; u += nthreads) {
-      const uint32_t r = __ldg(p.reorder + u);
-      int64_t val = -1;
-      if ((int64_t)r < p.nlv && (((__ldcg(vf + (r >> 5)) & ~__ldg(p.vis_init + (r >> 5))) >> (r & 31)) & 1u))
-        val = get_deferred<DEF>(p, r);
-      p.pred[u] = val;
-    }
+    for (int64_t u = tid; u < p.nolv; u += nthreads) p.pred[u] = final_entry<DEF>(p, __ldg(p.reorder + u));
     return;
   }
   for (int64_t u0 = tid * 4; u0 < p.nolv; u0 += nthreads * 4) {
     const uint4 ra = __ldcs(reinterpret_cast<const uint4*>(p.reorder + u0));
-    const uint32_t r[4] = {ra.x, ra.y, ra.z, ra.w};
     long long val[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      val[i] = -1ll;
-      if ((int64_t)r[i] < p.nlv) {
-        const uint32_t wv = __ldcg(vf + (r[i] >> 5)), wi = __ldg(p.vis_init + (r[i] >> 5));
-        const long long e = (long long)get_deferred<DEF>(p, r[i]);
-        if (((wv & ~wi) >> (r[i] & 31)) & 1u) val[i] = e;
-      }
-    }
+    val[0] = final_entry<DEF>(p, ra.x);
+    val[1] = final_entry<DEF>(p, ra.y);
+    val[2] = final_entry<DEF>(p, ra.z);
+    val[3] = final_entry<DEF>(p, ra.w);
     longlong2* dst = reinterpret_cast<longlong2*>(p.pred + u0);
     __stcs(dst, make_longlong2(val[0], val[1]));
     __stcs(dst + 1, make_longlong2(val[2], val[3]));
