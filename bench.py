@@ -61,6 +61,8 @@ def parse_args():
     ap.add_argument("--extra-scales", default="24,26",
                     help="graph sizes measured beside the main one (plain + batched), comma-separated; '' for none")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--partitioned-roots", type=int, default=8,
+                    help="N > 1: roots of the partitioned single-root BFS over all ranks (0: none)")
     ap.add_argument("--serve-scales", default="18,20,22,24")
     ap.add_argument("--serve-rates", default="1000,3000,10000,30000,100000")
     ap.add_argument("--serve-queries", type=int, default=10000)
@@ -499,6 +501,39 @@ def scale_section(a, g5, torch, scale, reduce_max, reduce_sum, barrier, peak) ->
     return out
 
 
+def partitioned_arm(a, g5, torch, dist, graph, roots, nedge, rank, world) -> dict:
+    """One BFS over all ranks (1-D partition, NCCL collectives every level):
+    each root validated, then timed by host wall clock between barriers, max
+    over ranks."""
+    from graph500_b200.partitioned import CudaRank, PartitionedBFS, TorchComm
+    dev = torch.device("cuda", torch.cuda.current_device())
+    bfs = PartitionedBFS(TorchComm(dist, dev), [CudaRank(graph, rank, world)], graph.info.num_global_verts,
+                         2000.0, 8.0)
+    rs = [int(r) for r in roots[:a.partitioned_roots]]
+    for i, r in enumerate(rs):
+        pred = bfs.run_bfs(r)
+        ok, evc, rep = g5.validate_bfs_result(graph, r, pred)
+        if not ok or evc != nedge[i]:
+            raise SystemExit(f"partitioned BFS: root {r} not valid ({rep}, {evc} vs {nedge[i]})")
+    ts = []
+    for r in rs:
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bfs.run_bfs(r)
+        torch.cuda.synchronize()
+        t = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ts.append(float(t.item()))
+    levels = len(bfs.levels)
+    bfs.close()
+    return {"workload": f"one BFS per root over {world} ranks (1-D vertex partition, NCCL all-to-all of top-down "
+                        f"pairs and all-gather of the bitmap every level), SCALE {a.scale}",
+            "value": sum(nedge[:len(rs)]) / sum(ts) / 1e9, "unit": UNIT, "roots": len(rs),
+            "ms_per_root": 1000.0 * sum(ts) / len(rs), "levels_last_root": levels,
+            "timing": "host wall clock between barriers, max over ranks", "parity": "every root validated"}
+
+
 def serving_arm(a, g5, torch, reduce_sum, barrier) -> dict:
     """Resident graphs at SCALE 18/20/22/24, open-loop Poisson queries (uniform
     graph, uniform degree>=1 root, splitmix64 seed 2026) at each rate; p50/p99
@@ -666,6 +701,9 @@ def our_arm(a):
 
     # batched multi-source BFS on the same graph and roots (one launch per 64 roots)
     batched = batched_arm(a, g5, torch, bfs, roots, nedge, pred_dev, local, reduce_max, reduce_sum, barrier)
+    partitioned = None
+    if world > 1 and a.partitioned_roots > 0:
+        partitioned = partitioned_arm(a, g5, torch, dist, bfs.graph_, roots, nedge, rank, world)
     peak, peak_kind = load_peaks()
     sections = {}
     for sc in [int(x) for x in a.extra_scales.split(",") if x]:
@@ -719,6 +757,8 @@ def our_arm(a):
     line["batched"] = batched
     line["batched"]["speedup_vs_plain"] = batched["value"] / value if value else None
     line.update(sections)
+    if partitioned is not None:
+        line["partitioned"] = partitioned
     if serving is not None:
         line["serving"] = serving
     if a.scale in cpu:
