@@ -332,7 +332,8 @@ def reference_arm(a):
             "warmup": a.warmup, "ms_per_step": 1000.0 * t / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic (Graph500 Kronecker generator, seeds 2/3)",
             "impl": "reference", "config": dict(workload(a), roots_per_step=per_step,
-                                                 parallelism="1 process, OpenMP"),
+                                                 parallelism="1 process, OpenMP",
+                                                 l2="not applicable: the reference runs on the host cores"),
             "harmonic_mean_gteps": hm / 1e9,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": rec["cores"], "kind": "reference",
                              "sample": f"{len(runs)} BFS runs ({per_step} roots/step) of the "
