@@ -63,7 +63,8 @@ constexpr uint32_t PACK_NONE = 0xFFFFFFFFu;
 constexpr int BFS_MIN_BLOCKS = 2;        // co-resident blocks per SM (64 registers, no spills)
 constexpr int TD_UNROLL = TD_CHUNK / 32;  // virtual edges per lane per pass
 constexpr int BU_WORDS = 4;               // 32-vertex words a warp keeps in flight (bottom-up pass A)
-constexpr int BU_SERIAL = 8;              // row entries a lane checks alone (one sector) before the warp helps
+constexpr int BU_SERIAL = 8;              // row entries a lane checks alone per step (one sector)
+constexpr int BU_LANE_MAX = 64;           // a row with at most this many entries left is scanned by its own lane
 // A frontier row of more than BIG_CHUNKS work items is listed whole (up to
 // BIG_ROWS rows per level) instead of cut into items by one warp; the next
 // top-down level spreads its chunks over every warp.
@@ -322,6 +323,29 @@ __device__ __forceinline__ bool vis_test(const uint32_t* __restrict__ vis, uint3
   return (__ldg(vis + (v >> 5)) >> (v & 31)) & 1u;
 }
 
+// One lane's next BU_SERIAL entries of its row from pos (loads first, then the
+// visited tests): the first entry visited before this level becomes the
+// parent and ends the row; k counts the entries examined.
+__device__ __forceinline__ void scan_serial(const RunParams& p, const uint32_t* __restrict__ vis_cur, uint64_t& pos,
+                                            uint64_t end, uint32_t& parent, uint32_t& k) {
+  uint32_t cv[BU_SERIAL];
+#pragma unroll
+  for (int t = 0; t < BU_SERIAL; ++t) cv[t] = pos + t < end ? __ldg(p.col + pos + t) : NO_VERTEX;
+  int hit_t = -1;
+#pragma unroll
+  for (int t = BU_SERIAL - 1; t >= 0; --t)
+    if (cv[t] != NO_VERTEX && vis_test(vis_cur, cv[t])) hit_t = t;
+  if (hit_t >= 0) {
+    parent = cv[hit_t];
+    k += (uint32_t)hit_t + 1;
+    pos = end;
+  } else {
+    const uint64_t adv = end - pos < (uint64_t)BU_SERIAL ? end - pos : (uint64_t)BU_SERIAL;
+    k += (uint32_t)adv;
+    pos += adv;
+  }
+}
+
 // Bottom-up level (bottom_up_search_bitmap, bfs.hpp:1839-2038), one warp per
 // 32 words of the visited bitmap at a time, both steps on the same words so
 // that no grid barrier separates them:
@@ -408,23 +432,15 @@ __device__ void bu_level(const RunParams& p, const uint32_t* __restrict__ vis_cu
         pos = __ldg(p.off + v) + 1;
         end = __ldg(p.off + v + 1);
         k = 1;
-        // the next BU_SERIAL entries: loads first, then the visited tests
-        uint32_t cv[BU_SERIAL];
-#pragma unroll
-        for (int t = 0; t < BU_SERIAL; ++t) cv[t] = pos + t < end ? __ldg(p.col + pos + t) : NO_VERTEX;
-        int hit_t = -1;
-#pragma unroll
-        for (int t = BU_SERIAL - 1; t >= 0; --t)
-          if (cv[t] != NO_VERTEX && vis_test(vis_cur, cv[t])) hit_t = t;
-        if (hit_t >= 0) {
-          parent = cv[hit_t];
-          k += (uint32_t)hit_t + 1;
-          pos = end;
-        } else {
-          const uint64_t adv = end - pos < (uint64_t)BU_SERIAL ? end - pos : (uint64_t)BU_SERIAL;
-          k += (uint32_t)adv;
-          pos += adv;
-        }
+        scan_serial(p, vis_cur, pos, end, parent, k);
+      }
+      // rows with at most BU_LANE_MAX entries left: every lane goes on along
+      // its own row, all rows at once (one warp-wide scan per row serialised
+      // the rows); longer rows are scanned by the whole warp below
+      for (;;) {
+        const bool mine = pos < end && end - pos <= (uint64_t)BU_LANE_MAX;
+        if (!__any_sync(FULL_MASK, mine)) break;
+        if (mine) scan_serial(p, vis_cur, pos, end, parent, k);
       }
       unsigned rest = __ballot_sync(FULL_MASK, pos < end);
       while (rest) {
