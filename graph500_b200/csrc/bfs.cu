@@ -99,6 +99,17 @@ struct RunParams {
 
 constexpr uint32_t FIRST_CHUNK = 0x80000000u;
 
+// pred = -1 except pred[root] = root (initialize_memory, bfs.hpp:241-276)
+__device__ __forceinline__ void fill_pred(const RunParams& p, int64_t tid, int64_t nthreads) {
+  if (!(reinterpret_cast<uintptr_t>(p.pred) & 15)) {  // 16-byte stores (nolv is even)
+    longlong2* pv = reinterpret_cast<longlong2*>(p.pred);
+    for (int64_t i = tid; i < p.nolv / 2; i += nthreads)
+      pv[i] = make_longlong2(2 * i == p.root ? p.root : -1, 2 * i + 1 == p.root ? p.root : -1);
+  } else {
+    for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = i == p.root ? p.root : -1;
+  }
+}
+
 // deferred modes (DEF = RunParams::deferred, a template argument of the
 // kernel so that each mode compiles to its own code): the entry of reordered
 // vertex r (parent's original id, level << 48)
@@ -559,24 +570,21 @@ __global__ void __launch_bounds__(BFS_THREADS, BFS_MIN_BLOCKS) bfs_persistent_ke
   if (tid == 0) ctl->t0_ns = globaltimer();
   // The root's own entries are written by the same fills, so one barrier
   // separates initialisation from the first level.
+  // The root's id comes first; the fills below do not wait for the loads
+  // that tell whether it has edges (pred is filled whether it has or not, and
+  // its bit in the visited map is set either way: without edges it is set
+  // already).
   const uint32_t root_r = p.reorder[p.root];
+  if (DEF == 0) fill_pred(p, tid, nthreads);
+  for (int64_t i = tid; i < p.nwords; i += nthreads)
+    p.vis[0][i] = p.vis_init[i] | ((int64_t)root_r < p.nlv && i == (int64_t)(root_r >> 5) ? 1u << (root_r & 31) : 0u);
   const bool has_edges = (int64_t)root_r < p.nlv && p.first[root_r] != NO_VERTEX;
   const uint64_t root_b = has_edges ? p.off[root_r] : 0;
   const uint64_t root_deg = has_edges ? p.off[root_r + 1] - root_b : 0;
   const int64_t root_items = (int64_t)chunks_of(root_deg);
-  if (DEF == 0 || !has_edges) {  // deferred mode writes pred whole at the end
-    if (!(reinterpret_cast<uintptr_t>(p.pred) & 15)) {  // 16-byte stores (nolv is even)
-      longlong2* pv = reinterpret_cast<longlong2*>(p.pred);
-      for (int64_t i = tid; i < p.nolv / 2; i += nthreads)
-        pv[i] = make_longlong2(2 * i == p.root ? p.root : -1, 2 * i + 1 == p.root ? p.root : -1);
-    } else {
-      for (int64_t i = tid; i < p.nolv; i += nthreads) p.pred[i] = i == p.root ? p.root : -1;
-    }
-  }
+  if (DEF != 0 && !has_edges) fill_pred(p, tid, nthreads);  // deferred mode writes pred whole at the end
   if constexpr (DEF != 0)
     if (has_edges && tid == 0) put_deferred<DEF>(p, root_r, (uint32_t)p.root, 0);
-  for (int64_t i = tid; i < p.nwords; i += nthreads)
-    p.vis[0][i] = p.vis_init[i] | (has_edges && i == (int64_t)(root_r >> 5) ? 1u << (root_r & 31) : 0u);
   if (blockIdx.x == 0 && threadIdx.x < 3 * C_NUM) (&ctl->cnt[0][0])[threadIdx.x] = 0;
   if (blockIdx.x == 0 && threadIdx.x < 3 * P_NUM) (&ctl->pos[0][0])[threadIdx.x] = 0;
 
