@@ -343,11 +343,15 @@ __device__ __forceinline__ void scan_serial(const RunParams& p, const uint32_t* 
 #pragma unroll
   for (int t = 0; t < BU_SERIAL; ++t) cv[t] = pos + t < end ? __ldg(p.col + pos + t) : NO_VERTEX;
   int hit_t = -1;
+  uint32_t hv = NO_VERTEX;  // cv[hit_t], kept as found: a dynamic index would put cv in local memory
 #pragma unroll
   for (int t = BU_SERIAL - 1; t >= 0; --t)
-    if (cv[t] != NO_VERTEX && vis_test(vis_cur, cv[t])) hit_t = t;
+    if (cv[t] != NO_VERTEX && vis_test(vis_cur, cv[t])) {
+      hit_t = t;
+      hv = cv[t];
+    }
   if (hit_t >= 0) {
-    parent = cv[hit_t];
+    parent = hv;
     k += (uint32_t)hit_t + 1;
     pos = end;
   } else {
