@@ -797,10 +797,14 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
       if (threadIdx.x < W && sh_lane[threadIdx.x]) atomicAdd(&ctl->lane_deg[threadIdx.x], sh_lane[threadIdx.x]);
       if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
       if (threadIdx.x < NW) {
+        uint32_t aw = 0;  // act.w[threadIdx.x], selected so that act stays in registers
+#pragma unroll
+        for (int k = 0; k < NW; ++k)
+          if (k == (int)threadIdx.x) aw = act.w[k];
         uint32_t q = 0;
         for (int b = 0; b < 32; ++b) {
           const int k = threadIdx.x * 32 + b;
-          if (((act.w[threadIdx.x] >> b) & 1u) && __ldcg(&ctl->lane_deg[k]) < survey_thr) q |= 1u << b;
+          if (((aw >> b) & 1u) && __ldcg(&ctl->lane_deg[k]) < survey_thr) q |= 1u << b;
         }
         sh_qm[threadIdx.x] = q;
       }
