@@ -184,6 +184,7 @@ def lib() -> C.CDLL:
         "g500_msbfs_wait": ([P, C.POINTER(MsStats)], i32),
         "g500_msbfs_set_root_stats": ([P, i32], i32),
         "g500_msbfs_set_grid": ([P, i32], i32),
+        "g500_msbfs_set_sparse": ([P, i32, i64], i32),
         "g500_msbfs_set_count": ([P, i32], i32),
         "g500_msbfs_get_grid": ([P, i32, C.POINTER(i32), C.POINTER(i32)], i32),
         "g500_msbfs_workspace_bytes": ([P, C.POINTER(u64)], i32),
@@ -571,6 +572,10 @@ class MultiSourceBFS:
 
     def set_grid(self, blocks: int = 0) -> None:
         check(lib().g500_msbfs_set_grid(self.h, blocks))
+
+    def set_sparse(self, on: bool = True, limit: int = 0) -> None:
+        """Sparse push levels up to a last-frontier degree sum of `limit` (0 = nlv / 8); levels are the same."""
+        check(lib().g500_msbfs_set_sparse(self.h, int(on), limit))
 
     def grid(self, lane_width: int = 64) -> tuple[int, int]:
         b, mx = C.c_int32(), C.c_int32()

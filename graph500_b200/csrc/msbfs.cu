@@ -71,6 +71,14 @@ struct MsParams {
   int64_t nhubs;
   const uint2* push_tab;     // push: [npush_chunks] the same for rows over MS_PUSH_HUB_DEG
   int64_t npush_chunks;
+  // Sparse levels.  fb[l % 3] marks the vertices whose frontier mask level l
+  // set (l = 0: the roots); `touched` marks the vertices a sparse push level
+  // gave N bits (clear between levels).  A push level is sparse when the last
+  // frontier's degree sum is at most sparse_limit.
+  uint32_t* fb[3];           // [3][nwords]
+  uint32_t* touched;         // [nwords]
+  int64_t nwords;            // (nlv + 31) / 32
+  int64_t sparse_limit;
   int64_t nlv;
   double alpha;
   MsCtl* ctl;
@@ -140,8 +148,8 @@ __device__ __forceinline__ bool covers(const Mask<NW>& acc, const Mask<NW>& need
   return ok;
 }
 
+constexpr int MS_GROUPS = 4;           // dense push: groups of 32 rows whose frontier masks load together
 constexpr int MS_WIN = 128;            // push: virtual edges a warp takes per window (4 per lane)
-constexpr int MS_GROUPS = 4;           // push: groups of 32 rows whose frontier masks load together
 constexpr int MS_SMALL_DEG = 128;      // pull: rows up to this long are walked by one thread
 constexpr int MS_UNROLL = 4;           // pull: neighbours each thread loads per step
 constexpr int MS_HUB_DEG = 1024;       // pull: rows longer than this are hub rows, split across warps
@@ -185,12 +193,15 @@ __device__ __forceinline__ unsigned long long sector_span(uint64_t b, uint64_t k
   return k ? ((b + k - 1) >> 3) - (b >> 3) + 1 : 0;
 }
 
-// Per-thread counters of a level, flushed once per block at its end.
+// Per-thread counters of a level, flushed once per block at its end; fb is
+// the level's frontier bitmap, track whether its push marks touched vertices.
 template <int NW>
 struct LevelAcc {
   unsigned long long nnew, nf, mf, mu;
   unsigned long long rows, sect;  // counting launches only
   Mask<NW> lanes;  // lanes that found vertices
+  uint32_t* fb;
+  bool track;
   __device__ void clear() {
     nnew = nf = mf = mu = rows = sect = 0;
 #pragma unroll
@@ -201,8 +212,9 @@ struct LevelAcc {
 // Vertex v (visited lanes vv, still-needed lanes need) found lanes nw this
 // level: its next-frontier mask (always written: the buffer holds an older
 // level), visited mask, level bytes and the counters of the direction rule.
+// Returns whether v found lanes (then it is marked in the level's frontier bitmap).
 template <int NW>
-__device__ __forceinline__ void settle(const MsParams& p, uint32_t* Fn, int64_t v, const Mask<NW>& vv,
+__device__ __forceinline__ bool settle(const MsParams& p, uint32_t* Fn, int64_t v, const Mask<NW>& vv,
                                        const Mask<NW>& need, const Mask<NW>& nw, uint32_t deg, uint32_t lvl4,
                                        LevelAcc<NW>& a) {
   constexpr int W = 32 * NW;
@@ -228,6 +240,7 @@ __device__ __forceinline__ void settle(const MsParams& p, uint32_t* Fn, int64_t 
     a.mf += deg;
   }
   if (left) a.mu += deg;  // still has unvisited live lanes after this level
+  return anynew;
 }
 
 // pull over non-hub rows.  A row of at most MS_SMALL_DEG edges is walked by
@@ -241,7 +254,7 @@ __device__ __forceinline__ void settle(const MsParams& p, uint32_t* Fn, int64_t 
 // INTO_N (a level that pulls some lanes and pushes the others): a row's
 // finds go into its next mask N, beside the push's, for the apply pass to
 // settle, instead of settling here.
-template <int NW, bool INTO_N, bool COUNT>
+template <int NW, bool INTO_N, bool COUNT, bool SP>
 __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, const uint32_t* Fc, uint32_t* Fn,
                              uint32_t lvl4, LevelAcc<NW>& la) {
   const int lane = threadIdx.x & 31;
@@ -334,6 +347,7 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, const uint3
       }
     }
     // hub rows settle after the hub phase (deg is 0 here for rows without needed lanes)
+    bool app = false;
     if (v < p.nlv && deg <= (uint32_t)MS_HUB_DEG) {
       Mask<NW> nw;
 #pragma unroll
@@ -343,8 +357,12 @@ __device__ void ms_pull_rows(const MsParams& p, const Mask<NW>& act, const uint3
         for (int k = 0; k < NW; ++k)
           if (nw.w[k]) atomicOr(p.N + v * NW + k, nw.w[k]);
       } else {
-        settle<NW>(p, Fn, v, vv, need, nw, deg, lvl4, la);
+        app = settle<NW>(p, Fn, v, vv, need, nw, deg, lvl4, la);
       }
+    }
+    if constexpr (SP && !INTO_N) {  // the warp's 32 vertices are one word of the frontier bitmap
+      const unsigned word = __ballot_sync(FULL_MASK, app);
+      if (lane == 0 && base < p.nlv) la.fb[base >> 5] = word;
     }
   }
 }
@@ -438,6 +456,23 @@ __device__ void ms_pull_hubs(const MsParams& p, const Mask<NW>& act, const uint3
   }
 }
 
+// The lanes of fo that w still lacks go into N[w]; with track, w is marked
+// touched when it got some.
+template <int NW>
+__device__ __forceinline__ void push_to(const MsParams& p, uint32_t w, const Mask<NW>& fo, bool track) {
+  const Mask<NW> vw = load_mask<NW>(p.V + (int64_t)w * NW);
+  bool any = false;
+#pragma unroll
+  for (int q = 0; q < NW; ++q) {
+    const uint32_t add = fo.w[q] & ~vw.w[q];
+    if (add) {
+      atomicOr(p.N + (int64_t)w * NW + q, add);
+      any = true;
+    }
+  }
+  if (any && track) atomicOr(p.touched + (w >> 5), 1u << (w & 31));
+}
+
 // push from hub frontier rows: every neighbour of the chunk gets the lanes it
 // still lacks
 template <int NW, bool COUNT>
@@ -485,25 +520,19 @@ __device__ void ms_push_hubs(const MsParams& p, const uint32_t* Fc, const Mask<N
         }
 #pragma unroll
         for (int t = 0; t < MS_UNROLL; ++t)
-          if (nb[t] != NO_VERTEX) {
-            const Mask<NW> vw = load_mask<NW>(p.V + (int64_t)nb[t] * NW);
-#pragma unroll
-            for (int q = 0; q < NW; ++q) {
-              const uint32_t add = fo.w[q] & ~vw.w[q];
-              if (add) atomicOr(p.N + (int64_t)nb[t] * NW + q, add);
-            }
-          }
+          if (nb[t] != NO_VERTEX) push_to<NW>(p, nb[t], fo, la.track);
       }
     }
   }
 }
 
-// push from non-hub frontier rows: the frontier masks of MS_GROUPS groups of
+// push from non-hub frontier rows (graphs without sparse levels: every
+// vertex's frontier mask is read): the frontier masks of MS_GROUPS groups of
 // 32 rows are loaded together; each group holding frontier rows has their
 // edges walked as one list, MS_WIN at a time; every neighbour gets the lanes
 // it still lacks.
 template <int NW, bool COUNT>
-__device__ void ms_push_rows(const MsParams& p, const uint32_t* Fc, const Mask<NW>& qm, LevelAcc<NW>& la) {
+__device__ void ms_push_rows_dense(const MsParams& p, const uint32_t* Fc, const Mask<NW>& qm, LevelAcc<NW>& la) {
   const int lane = threadIdx.x & 31;
   for (int64_t base = gwarp_id() * (32 * MS_GROUPS); base < p.nlv; base += gwarp_count() * (32 * MS_GROUPS)) {
     Mask<NW> fg[MS_GROUPS];
@@ -569,15 +598,86 @@ __device__ void ms_push_rows(const MsParams& p, const uint32_t* Fc, const Mask<N
   }
 }
 
+// push from non-hub frontier rows: the rows marked in fbc (the last level's
+// frontier bitmap), gathered 32 at a time from each warp's 32 words, so that
+// a small frontier costs a pass over its bitmap and not over every vertex;
+// each batch of rows has its edges walked as one list, MS_WIN at a time;
+// every neighbour gets the lanes it still lacks.
+template <int NW, bool COUNT>
+__device__ void ms_push_rows_marked(const MsParams& p, const uint32_t* Fc, const uint32_t* fbc, const Mask<NW>& qm,
+                             LevelAcc<NW>& la) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t wb = gwarp_id() * 32; wb < p.nwords; wb += gwarp_count() * 32) {
+    const int64_t wi = wb + lane;
+    const uint32_t mw = wi < p.nwords ? __ldcg(fbc + wi) : 0u;
+    const uint32_t c = __popc(mw);
+    const uint32_t incl_w = warp_incl_scan(c);
+    const uint32_t excl_w = incl_w - c;
+    const uint32_t nrows = __shfl_sync(FULL_MASK, incl_w, 31);
+    for (uint32_t b0 = 0; b0 < nrows; b0 += 32) {
+      const uint32_t idx = b0 + lane;
+      const int ow = owner_lane(excl_w, idx);
+      const uint32_t mwo = __shfl_sync(FULL_MASK, mw, ow);
+      const uint32_t exw = __shfl_sync(FULL_MASK, excl_w, ow);
+      Mask<NW> f;
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) f.w[k] = 0;
+      uint64_t cur = 0, re = 0;
+      if (idx < nrows) {
+        const int64_t v = (wb + ow) * 32 + select_bit(mwo, idx - exw);
+        f = load_mask<NW>(Fc + v * NW);
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+          f.w[k] &= qm.w[k];
+          any |= f.w[k] != 0;
+        }
+        if (any) {
+          cur = __ldg(p.off + v);
+          re = cur + __ldg(p.deg + v);
+          if (re - cur > (uint64_t)MS_PUSH_HUB_DEG) cur = re;  // hub row: the hub phase pushes it
+          if constexpr (COUNT)
+            if (re > cur) {
+              ++la.rows;
+              la.sect += sector_span(cur, re - cur);
+            }
+        }
+      }
+      for (;;) {
+        const uint32_t rem = (uint32_t)((re - cur) < (uint64_t)MS_WIN ? (re - cur) : (uint64_t)MS_WIN);
+        const uint32_t incl = warp_incl_scan(rem);
+        const uint32_t excl = incl - rem;
+        const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
+        if (total == 0) break;
+#pragma unroll
+        for (int j = 0; j < MS_WIN / 32; ++j) {
+          const uint32_t k = j * 32 + lane;
+          const int o = owner_lane(excl, k);
+          const uint64_t co = __shfl_sync(FULL_MASK, cur, o);
+          const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
+          Mask<NW> fo;
+#pragma unroll
+          for (int q = 0; q < NW; ++q) fo.w[q] = __shfl_sync(FULL_MASK, f.w[q], o);
+          if (k < total) push_to<NW>(p, __ldg(p.col + co + (k - exo)), fo, la.track);
+        }
+        cur += excl >= (uint32_t)MS_WIN ? 0u : min(rem, (uint32_t)MS_WIN - excl);
+      }
+    }
+  }
+}
+
 // apply after a push level: new = N & needed lanes; settle every vertex (its
 // next-frontier mask is always written).  U vertices per thread per step,
-// loads first.
-template <int NW>
+// loads first; each warp's 32 vertices of a step are one word of the
+// frontier bitmap.
+template <int NW, bool SP>
 __device__ void ms_apply(const MsParams& p, const Mask<NW>& act, uint32_t* Fn, uint32_t lvl4, LevelAcc<NW>& la) {
   constexpr int U = NW == 4 ? 2 : 4;
+  const int lane = threadIdx.x & 31;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t v0 = tid; v0 < p.nlv; v0 += nthreads * U) {
+  for (int64_t v0w = tid - lane; v0w < p.nlv; v0w += nthreads * U) {  // v0w: the warp's first vertex (uniform)
+    const int64_t v0 = v0w + lane;
     Mask<NW> n[U], vv[U];
     uint32_t dg[U];
 #pragma unroll
@@ -596,28 +696,99 @@ __device__ void ms_apply(const MsParams& p, const Mask<NW>& act, uint32_t* Fn, u
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t v = v0 + u * nthreads;
-      if (v >= p.nlv) continue;
-      Mask<NW> need, nw;
-      bool anyn = false;
+      bool app = false;
+      if (v < p.nlv) {
+        Mask<NW> need, nw;
+        bool anyn = false;
 #pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        need.w[k] = act.w[k] & ~vv[u].w[k];
-        nw.w[k] = n[u].w[k] & need.w[k];
-        anyn |= n[u].w[k] != 0;
+        for (int k = 0; k < NW; ++k) {
+          need.w[k] = act.w[k] & ~vv[u].w[k];
+          nw.w[k] = n[u].w[k] & need.w[k];
+          anyn |= n[u].w[k] != 0;
+        }
+        if (anyn) {
+          Mask<NW> zero;
+#pragma unroll
+          for (int k = 0; k < NW; ++k) zero.w[k] = 0;
+          store_mask<NW>(p.N + v * NW, zero);
+        }
+        app = settle<NW>(p, Fn, v, vv[u], need, nw, dg[u], lvl4, la);
       }
-      if (anyn) {
-        Mask<NW> zero;
+      if constexpr (SP) {
+        const unsigned word = __ballot_sync(FULL_MASK, app);
+        const int64_t vw = v0w + u * nthreads;  // a multiple of 32
+        if (lane == 0 && vw < p.nlv) la.fb[vw >> 5] = word;
+      }
+    }
+  }
+}
+
+// apply after a sparse push level: only the touched vertices have N bits, so
+// only they settle (each warp gathers the marked vertices of its 32 words,
+// 32 at a time, and clears the words); every other vertex's next-frontier
+// mask is clear already (the push phase cleared the masks the buffer held
+// from two levels before, and this level's frontier bitmap).  Mu, the degree
+// sum of vertices with needed lanes left, is not summed here (the caller
+// keeps the last one).
+template <int NW>
+__device__ void ms_apply_marked(const MsParams& p, const Mask<NW>& act, uint32_t* Fn, uint32_t lvl4,
+                                LevelAcc<NW>& la) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t wb = gwarp_id() * 32; wb < p.nwords; wb += gwarp_count() * 32) {
+    const int64_t wi = wb + lane;
+    const uint32_t mw = wi < p.nwords ? __ldcg(p.touched + wi) : 0u;
+    if (mw) p.touched[wi] = 0;
+    const uint32_t c = __popc(mw);
+    const uint32_t incl = warp_incl_scan(c);
+    const uint32_t excl = incl - c;
+    const uint32_t total = __shfl_sync(FULL_MASK, incl, 31);
+    for (uint32_t b0 = 0; b0 < total; b0 += 32) {
+      const uint32_t idx = b0 + lane;
+      const int o = owner_lane(excl, idx);
+      const uint32_t mwo = __shfl_sync(FULL_MASK, mw, o);
+      const uint32_t exo = __shfl_sync(FULL_MASK, excl, o);
+      if (idx < total) {
+        const int64_t v = (wb + o) * 32 + select_bit(mwo, idx - exo);
+        const Mask<NW> n = load_mask<NW>(p.N + v * NW);
+        const Mask<NW> vv = load_mask<NW>(p.V + v * NW);
+        Mask<NW> need, nw, zero;
 #pragma unroll
-        for (int k = 0; k < NW; ++k) zero.w[k] = 0;
+        for (int k = 0; k < NW; ++k) {
+          need.w[k] = act.w[k] & ~vv.w[k];
+          nw.w[k] = n.w[k] & need.w[k];
+          zero.w[k] = 0;
+        }
         store_mask<NW>(p.N + v * NW, zero);
+        if (settle<NW>(p, Fn, v, vv, need, nw, __ldg(p.deg + v), lvl4, la))
+          atomicOr(la.fb + (v >> 5), 1u << (v & 31));
       }
-      settle<NW>(p, Fn, v, vv[u], need, nw, dg[u], lvl4, la);
+    }
+  }
+}
+
+// the next-frontier masks of the vertices marked in fb_old (the level two
+// before, whose masks the buffer still holds) cleared, and fb_new (this
+// level's frontier bitmap, last written three levels before) cleared
+template <int NW>
+__device__ void ms_clear_marked(const MsParams& p, uint32_t* Fn, const uint32_t* fb_old, uint32_t* fb_new) {
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  Mask<NW> zero;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) zero.w[k] = 0;
+  for (int64_t wi = tid; wi < p.nwords; wi += nthreads) {
+    uint32_t m = fb_old ? __ldcg(fb_old + wi) : 0u;
+    fb_new[wi] = 0;
+    while (m) {
+      const int b = __ffs(m) - 1;
+      m &= m - 1;
+      store_mask<NW>(Fn + (wi * 32 + b) * NW, zero);
     }
   }
 }
 
 // after a pull level: the hub rows, whose chunks ORed into N
-template <int NW>
+template <int NW, bool SP>
 __device__ void ms_settle_hubs(const MsParams& p, const Mask<NW>& act, uint32_t* Fn, uint32_t lvl4,
                                LevelAcc<NW>& la) {
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -640,7 +811,9 @@ __device__ void ms_settle_hubs(const MsParams& p, const Mask<NW>& act, uint32_t*
       for (int k = 0; k < NW; ++k) zero.w[k] = 0;
       store_mask<NW>(p.N + (int64_t)h * NW, zero);
     }
-    settle<NW>(p, Fn, h, vv, need, nw, __ldg(p.deg + h), lvl4, la);
+    const bool app = settle<NW>(p, Fn, h, vv, need, nw, __ldg(p.deg + h), lvl4, la);
+    if constexpr (SP)
+      if (app) atomicOr(la.fb + (h >> 5), 1u << (h & 31));  // the pull phase wrote its bit clear
   }
 }
 
@@ -715,7 +888,9 @@ __device__ void flush_level(const LevelAcc<NW>& la, unsigned long long* sh_acc, 
 // COUNT: a counting launch, which also records each level's offset reads and
 // adjacency sectors (the bytes model of the batched form); compiled apart so
 // that the timed launches carry none of it.
-template <int NW, bool COUNT>
+// SP: sparse levels (frontier and touched bitmaps) are kept; without, every
+// level works on every vertex (smaller graphs, where that costs less).
+template <int NW, bool COUNT, bool SP>
 __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsParams p) {
   constexpr int W = 32 * NW;
   __shared__ unsigned long long sh_cnt[M_NUM];
@@ -737,11 +912,17 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
     Mask<NW> zero;
 #pragma unroll
     for (int k = 0; k < NW; ++k) zero.w[k] = 0;
-    for (int64_t v = tid; v < p.nlv; v += nthreads) {  // F[1] is written whole by level 1
-      store_mask<NW>(p.V + v * NW, zero);
+    for (int64_t v = tid; v < p.nlv; v += nthreads) {  // SP: level 1 may settle only the vertices it touches
+      store_mask<NW>(p.V + v * NW, zero);               // (otherwise F[1] is written whole by level 1)
       store_mask<NW>(p.F[0] + v * NW, zero);
+      if constexpr (SP) store_mask<NW>(p.F[1] + v * NW, zero);
       store_mask<NW>(p.N + v * NW, zero);
     }
+    if constexpr (SP)
+      for (int64_t w = tid; w < p.nwords; w += nthreads) {
+        p.touched[w] = 0;
+        p.fb[0][w] = 0;
+      }
   }
   if (blockIdx.x == 0 && threadIdx.x < 3 * M_NUM) (&ctl->cnt[0][0])[threadIdx.x] = 0;
   if (blockIdx.x == 0 && threadIdx.x < 12) (&ctl->alive[0][0])[threadIdx.x] = 0;
@@ -755,6 +936,7 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
       atomicOr(p.V + (int64_t)r * NW + tid / 32, 1u << (tid & 31));
       atomicOr(p.F[0] + (int64_t)r * NW + tid / 32, 1u << (tid & 31));
       p.L[(int64_t)r * W + tid] = 0;
+      if constexpr (SP) atomicOr(p.fb[0] + (r >> 5), 1u << (r & 31));  // level 0's frontier bitmap
     }
   }
   if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
@@ -767,6 +949,8 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
   __shared__ unsigned long long sh_lane[MS_MAX_LANES];
   __shared__ uint32_t sh_qm[4];
   const unsigned long long survey_thr = __ldg(p.off + p.nlv) / ((unsigned long long)MS_SURVEY_DIV * MS_SURVEY_STEP);
+  unsigned long long mu_last = __ldg(p.off + p.nlv);  // every vertex needs every lane
+  unsigned long long mf_last = 0;                     // level 1: the roots' rows
   for (;; ++level) {
     unsigned long long* cnt = ctl->cnt[phase % 3];
     unsigned* alive = ctl->alive[phase % 3];
@@ -777,6 +961,7 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
     const uint32_t lvl4 = (uint32_t)level * 0x01010101u;
     LevelAcc<NW> la;
     la.clear();
+    la.fb = p.fb[level % 3];
     // The first level that would pull surveys the lanes' frontiers: lanes
     // whose frontier degree sum is under 1/MS_SURVEY_DIV of the graph's entries are
     // pushed at that level, the others pulled (a mixed level: both phases
@@ -823,17 +1008,29 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
 #pragma unroll
       for (int k = 0; k < NW; ++k) mixed |= qm.w[k] != 0;
     }
+    // A push level is sparse when the last frontier's degree sum (which
+    // bounds the vertices it can touch) is at most sparse_limit: it marks the
+    // vertices it touches and settles only those, after clearing, during the
+    // push, the masks Fn still holds from two levels before (marked in that
+    // level's frontier bitmap) and its own frontier bitmap.
+    const bool sparse = SP && !pull && !mixed && (int64_t)mf_last <= p.sparse_limit;
+    const uint32_t* fbc = p.fb[(level - 1) % 3];
+    la.track = sparse;
     if (pull && !mixed) {
-      ms_pull_rows<NW, false, COUNT>(p, act, Fc, Fn, lvl4, la);
+      ms_pull_rows<NW, false, COUNT, SP>(p, act, Fc, Fn, lvl4, la);
       ms_pull_hubs<NW, COUNT>(p, act, Fc, la);
     } else if (mixed) {
-      ms_push_rows<NW, COUNT>(p, Fc, qm, la);
+      if constexpr (SP) ms_push_rows_marked<NW, COUNT>(p, Fc, fbc, qm, la);
+      else ms_push_rows_dense<NW, COUNT>(p, Fc, qm, la);
       ms_push_hubs<NW, COUNT>(p, Fc, qm, la);
-      ms_pull_rows<NW, true, COUNT>(p, pm, Fc, Fn, lvl4, la);
+      ms_pull_rows<NW, true, COUNT, SP>(p, pm, Fc, Fn, lvl4, la);
       ms_pull_hubs<NW, COUNT>(p, pm, Fc, la);
     } else {
-      ms_push_rows<NW, COUNT>(p, Fc, qm, la);
+      if constexpr (SP) ms_push_rows_marked<NW, COUNT>(p, Fc, fbc, qm, la);
+      else ms_push_rows_dense<NW, COUNT>(p, Fc, qm, la);
       ms_push_hubs<NW, COUNT>(p, Fc, qm, la);
+      // (level 1: Fn is clear from the start)
+      if (sparse) ms_clear_marked<NW>(p, Fn, level > 1 ? p.fb[(level - 2) % 3] : nullptr, la.fb);
     }
     pulls += pull;
     if (!grid_sync<M_NUM>(&ctl->bar, nullptr, sh_acc, nullptr, sh_cnt, &sh_flag)) return;
@@ -842,8 +1039,9 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
     // survey adds after the level's closing one
     if (survey && blockIdx.x == 0)
       for (int i = threadIdx.x; i < MS_MAX_LANES; i += blockDim.x) ctl->lane_deg[i] = 0;
-    if (pull && !mixed) ms_settle_hubs<NW>(p, act, Fn, lvl4, la);
-    else ms_apply<NW>(p, act, Fn, lvl4, la);
+    if (pull && !mixed) ms_settle_hubs<NW, SP>(p, act, Fn, lvl4, la);
+    else if (sparse) ms_apply_marked<NW>(p, act, Fn, lvl4, la);
+    else ms_apply<NW, SP>(p, act, Fn, lvl4, la);
     flush_level<NW, COUNT>(la, sh_acc, sh_or, alive);
     if (!grid_sync_sum<M_NUM>(cnt, &ctl->bar, sh_acc, sh_cnt)) return;
     ++phase;
@@ -868,7 +1066,10 @@ __global__ void __launch_bounds__(MS_THREADS, MS_MIN_BLOCKS) msbfs_kernel(MsPara
       if (tid == 0) atomicOr(&ctl->bar.err, (unsigned)MS_ERR_DEPTH);
       break;
     }
-    pull = (double)sh_cnt[M_MF] > (double)sh_cnt[M_MU] / p.alpha;
+    const unsigned long long mu = sparse ? mu_last : sh_cnt[M_MU];
+    mu_last = mu;
+    mf_last = sh_cnt[M_MF];
+    pull = (double)sh_cnt[M_MF] > (double)mu / p.alpha;
   }
   if (tid == 0) {
     ctl->num_levels = (unsigned)level;
@@ -1073,6 +1274,9 @@ struct g500_msbfs {
   int64_t nhub_rows = 0;
   uint2* push_tab = nullptr;                          // push: [npush_chunks]
   int64_t npush_chunks = 0;
+  uint32_t* marks = nullptr;                          // [4][nwords]: three frontier bitmaps, the touched bitmap
+  int64_t nwords = 0;
+  int64_t sparse_limit = 0;                           // g500_msbfs_set_sparse (-1: never sparse)
   int last_nroots = 0;
   int last_batches = 0;
 };
@@ -1106,6 +1310,7 @@ static int ms_free(g500_msbfs* m) {
   dev_free(m->hub_tab);
   dev_free(m->hub_rows);
   dev_free(m->push_tab);
+  dev_free(m->marks);
   if (m->staging) cudaFreeHost(m->staging);
   if (m->h_ctl) cudaFreeHost(m->h_ctl);
   if (m->h_stats) cudaFreeHost(m->h_stats);
@@ -1118,7 +1323,7 @@ static int ms_free(g500_msbfs* m) {
 }
 
 template <int NW>
-static const void* ms_kernel_ptr() { return (const void*)msbfs_kernel<NW, false>; }
+static const void* ms_kernel_ptr() { return (const void*)msbfs_kernel<NW, false, true>; }
 
 // Chunk table of the rows longer than `thresh`, `chunk` edges per chunk, so
 // that warps can share a hub's row.
@@ -1214,6 +1419,10 @@ static int ms_enqueue_batch(g500_msbfs* m, int b, cudaStream_t s) {
   p.nhub_chunks = m->nhub_chunks;
   p.push_tab = m->push_tab;
   p.npush_chunks = m->npush_chunks;
+  for (int i = 0; i < 3; ++i) p.fb[i] = m->marks + i * m->nwords;
+  p.touched = m->marks + 3 * m->nwords;
+  p.nwords = m->nwords;
+  p.sparse_limit = m->sparse_limit;
   p.alpha = m->alpha;
   p.ctl = m->ctl + b;
   cudaLaunchConfig_t cfg = {};
@@ -1225,14 +1434,15 @@ static int ms_enqueue_batch(g500_msbfs* m, int b, cudaStream_t s) {
   attr.val.cooperative = 1;
   cfg.attrs = &attr;
   cfg.numAttrs = 1;
+  const bool sp = m->sparse_limit >= 0;
   if (m->count) {  // the counting variant has the timed kernel's grid (same launch bounds)
-    if (W == 32) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<1, true>, p));
-    else if (W == 64) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<2, true>, p));
-    else G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<4, true>, p));
+    if (W == 32) G500_CUDA(cudaLaunchKernelEx(&cfg, sp ? msbfs_kernel<1, true, true> : msbfs_kernel<1, true, false>, p));
+    else if (W == 64) G500_CUDA(cudaLaunchKernelEx(&cfg, sp ? msbfs_kernel<2, true, true> : msbfs_kernel<2, true, false>, p));
+    else G500_CUDA(cudaLaunchKernelEx(&cfg, sp ? msbfs_kernel<4, true, true> : msbfs_kernel<4, true, false>, p));
   } else {
-    if (W == 32) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<1, false>, p));
-    else if (W == 64) G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<2, false>, p));
-    else G500_CUDA(cudaLaunchKernelEx(&cfg, msbfs_kernel<4, false>, p));
+    if (W == 32) G500_CUDA(cudaLaunchKernelEx(&cfg, sp ? msbfs_kernel<1, false, true> : msbfs_kernel<1, false, false>, p));
+    else if (W == 64) G500_CUDA(cudaLaunchKernelEx(&cfg, sp ? msbfs_kernel<2, false, true> : msbfs_kernel<2, false, false>, p));
+    else G500_CUDA(cudaLaunchKernelEx(&cfg, sp ? msbfs_kernel<4, false, true> : msbfs_kernel<4, false, false>, p));
   }
   uint8_t* out = m->out + (int64_t)b * W * g->nolv;
   const unsigned tg = (unsigned)std::min<int64_t>(ceil_div(g->nolv, 4 * TR_BLOCK), (int64_t)num_sms() * 8);
@@ -1260,6 +1470,13 @@ extern "C" int g500_msbfs_create(g500_graph* g, g500_msbfs** out) {
   if (st == G500_OK) st = dev_alloc_n(&m->N, nlv * 4, "msbfs next masks");
   if (st == G500_OK) st = dev_alloc_n(&m->L, nlv * MS_MAX_LANES, "msbfs levels");
   if (st == G500_OK) st = dev_alloc_n(&m->deg, nlv, "msbfs row lengths");
+  // sparse levels: frontier and touched bitmaps; from 2^22 vertices with
+  // edges, a push level is sparse up to a last-frontier degree sum of nlv / 8
+  // (on smaller graphs a pass over every vertex costs less than the sparse
+  // level's extra steps)
+  m->nwords = (nlv + 31) / 32;
+  m->sparse_limit = nlv >= (int64_t(1) << 22) ? nlv / 8 : -1;
+  if (st == G500_OK) st = dev_alloc_n(&m->marks, 4 * m->nwords, "msbfs frontier and touched bitmaps");
   if (st == G500_OK && g->nlv > 0) {
     const unsigned dgrid = (unsigned)std::min<int64_t>(ceil_div(g->nlv, 256), (int64_t)num_sms() * 8);
     ms_degree_kernel<<<dgrid, 256, 0, m->stream>>>(g->d_offsets, g->nlv, m->deg);
@@ -1490,6 +1707,18 @@ extern "C" int g500_msbfs_set_grid(g500_msbfs* m, int blocks) {
   return G500_OK;
 }
 
+extern "C" int g500_msbfs_set_sparse(g500_msbfs* m, int on, int64_t limit) {
+  if (!m) return set_error(G500_E_INVAL, "null handle");
+  if (limit < 0) return set_error(G500_E_INVAL, "negative degree-sum limit");
+  if (m->in_flight) return set_error(G500_E_STATE, "a launch is in flight");
+  const int64_t want = !on ? -1 : (limit == 0 ? std::max<int64_t>(std::max<int64_t>(m->g->nlv, 1) / 8, 1) : limit);
+  if (want != m->sparse_limit) {
+    ms_drop_graphs(m);  // the captured launches carry the limit
+    m->sparse_limit = want;
+  }
+  return G500_OK;
+}
+
 extern "C" int g500_msbfs_get_grid(const g500_msbfs* m, int lane_width, int* blocks, int* max_blocks) {
   if (!m) return set_error(G500_E_INVAL, "null handle");
   if (lane_width != 32 && lane_width != 64 && lane_width != 128)
@@ -1502,10 +1731,11 @@ extern "C" int g500_msbfs_get_grid(const g500_msbfs* m, int lane_width, int* blo
 extern "C" int g500_msbfs_workspace_bytes(const g500_graph* g, uint64_t* bytes) {
   if (!g || !bytes) return set_error(G500_E_INVAL, "null argument");
   const uint64_t nlv = (uint64_t)std::max<int64_t>(g->nlv, 1);
-  // V, F, N (4 words each), L (128 bytes), row lengths, output rows, with room
-  // for the hub tables and control blocks
+  // V, F, N (4 words each), L (128 bytes), row lengths, output rows, the
+  // sparse-level bitmaps (4 bits), with room for the hub tables and control
+  // blocks
   *bytes = nlv * (4 * 16 + MS_MAX_LANES + 4) + (uint64_t)MS_MAX_LANES * (uint64_t)g->nolv + (16ull << 20) +
-           (uint64_t)g->nge / 64;
+           (uint64_t)g->nge / 64 + (nlv + 31) / 32 * 16;
   return G500_OK;
 }
 

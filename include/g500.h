@@ -329,6 +329,12 @@ int g500_msbfs_set_root_stats(g500_msbfs* m, int on);
  * blocks leave SMs to launches of other handles running at the same time. */
 int g500_msbfs_set_grid(g500_msbfs* m, int blocks);
 int g500_msbfs_get_grid(const g500_msbfs* m, int lane_width, int* blocks, int* max_blocks);
+/* Sparse levels: a push level whose last frontier has a degree sum of at most
+ * `limit` (0 = nlv / 8) works on the marked vertices only (the frontier rows
+ * and the vertices it touches) instead of every vertex; on = 0 makes every
+ * level dense.  Default: on with nlv / 8 from 2^22 vertices with edges, off
+ * below.  The levels are the same either way. */
+int g500_msbfs_set_sparse(g500_msbfs* m, int on, int64_t limit);
 /* Device memory one handle on this graph allocates (an upper bound). */
 int g500_msbfs_workspace_bytes(const g500_graph* g, uint64_t* bytes);
 /* Autotuner over lane width and alpha on sample roots (kept on the handle). */

@@ -39,6 +39,26 @@ def test_msbfs_levels_bit_exact(g500, s13, lane_width, use_graph, alpha):
     ms.close()
 
 
+@pytest.mark.parametrize("lane_width", [32, 64, 128])
+@pytest.mark.parametrize("sparse,limit", [(False, 0), (True, 1), (True, 300), (True, 0), (True, 1 << 40)])
+def test_msbfs_sparse_levels_keep_levels(g500, s13, lane_width, sparse, limit):
+    """Dense levels only, sparse push levels for small frontiers (limits 1 and
+    300 put the switch between the two inside the search), and every push
+    level sparse: the same levels.  alpha 1e-12 pushes every level; 15 mixes
+    push and pull levels."""
+    g, og, roots, want = s13
+    ms = g500.MultiSourceBFS(g, lane_width, 15.0, True)
+    ms.set_sparse(sparse, limit)
+    for alpha in (1e-12, 15.0):
+        ms.set_params(lane_width, alpha, True)
+        for n in (len(roots), 5):
+            assert np.array_equal(ms.levels(roots[:n]), want[:n]), (lane_width, sparse, limit, alpha, n)
+    with pytest.raises(g500.G500Error) as ei:
+        ms.set_sparse(True, -1)
+    assert ei.value.code == g500.G500_E_INVAL
+    ms.close()
+
+
 def test_msbfs_repeated_runs_and_device_output(g500, s13):
     import torch
     g, og, roots, want = s13
