@@ -150,10 +150,19 @@ __device__ __forceinline__ bool covers(const Mask<NW>& acc, const Mask<NW>& need
 
 constexpr int MS_GROUPS = 4;           // dense push: groups of 32 rows whose frontier masks load together
 constexpr int MS_WIN = 128;            // push: virtual edges a warp takes per window (4 per lane)
-constexpr int MS_SMALL_DEG = 128;      // pull: rows up to this long are walked by one thread
+// Pull: rows up to MS_SMALL_DEG entries are walked by one thread, longer ones
+// by a whole warp with a coverage check per step, and only rows of more than
+// MS_HUB_DEG entries are split into chunks for several warps.  A chunk is
+// scanned to its end whatever the row's coverage, while a walked row stops as
+// soon as its needed lanes are found (at once for most high-degree rows), so
+// splitting pays only for the very largest rows: with hub rows from 1024
+// entries (1024-entry chunks) and single-thread rows up to 128, 64 roots took
+// 1010 / 3719 / 16090 us at SCALE 22 / 24 / 26, against 894 / 2971 / 11349 us
+// with these values.
+constexpr int MS_SMALL_DEG = 256;      // pull: rows up to this long are walked by one thread
 constexpr int MS_UNROLL = 4;           // pull: neighbours each thread loads per step
-constexpr int MS_HUB_DEG = 1024;       // pull: rows longer than this are hub rows, split across warps
-constexpr int MS_HUB_CHUNK = 1024;     // pull: edges of a hub row one warp takes at a time
+constexpr int MS_HUB_DEG = 1 << 20;    // pull: rows longer than this are hub rows, split across warps
+constexpr int MS_HUB_CHUNK = 16384;    // pull: edges of a hub row one warp takes at a time
 constexpr int MS_PUSH_HUB_DEG = 256;   // push: the same two, smaller: a push walks every edge of its
 constexpr int MS_PUSH_CHUNK = 256;     //   frontier rows, so short chunks spread the few hub rows wider
 

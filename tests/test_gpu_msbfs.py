@@ -124,6 +124,42 @@ def test_msbfs_autotune_keeps_levels(g500, s13):
     ms.close()
 
 
+@pytest.fixture(scope="module")
+def star(g500, oracle_mod):
+    """A star whose centre has more than 2^20 neighbours (a hub row for both
+    the pull and the push phase), a 40-vertex path hanging off one leaf, and
+    2000 random edges among the leaves."""
+    leaves = (1 << 20) + 300
+    rng = np.random.default_rng(7)
+    pairs = [np.stack([np.zeros(leaves, np.int64), np.arange(1, leaves + 1)], 1)]
+    path = np.arange(leaves + 1, leaves + 41)
+    pairs.append(np.stack([np.concatenate([[5], path[:-1]]), path], 1))
+    pairs.append(rng.integers(1, leaves + 1, (2000, 2)))
+    pr = np.concatenate(pairs)
+    edges = np.zeros(len(pr), g500.EDGE_DTYPE)
+    edges["v0_low"], edges["v1_low"] = pr[:, 0], pr[:, 1]
+    og = oracle_mod.Graph(edges, 2)
+    g = g500.Graph2DCSR.build(edges, 2)
+    roots = np.array([0, 5, int(path[-1]), int(path[20]), 17, 123456, leaves], np.int64)
+    want = np.stack([as_u8(og.bfs_levels(int(r))) for r in roots])
+    yield g, roots, want
+    g.close()
+
+
+@pytest.mark.parametrize("lane_width", [32, 128])
+@pytest.mark.parametrize("alpha", [1e-12, 1e12])
+@pytest.mark.parametrize("sparse", [False, True])
+def test_msbfs_hub_rows_keep_levels(g500, star, lane_width, alpha, sparse):
+    """Rows longer than the hub thresholds are split into chunks that several
+    warps take (push: over 256 entries, pull: over 2^20); alpha 1e-12 pushes
+    every level and 1e12 pulls every level after the first."""
+    g, roots, want = star
+    ms = g500.MultiSourceBFS(g, lane_width, alpha, True)
+    ms.set_sparse(sparse, 0)
+    assert np.array_equal(ms.levels(roots), want), (lane_width, alpha, sparse)
+    ms.close()
+
+
 def test_msbfs_refuses_depth_beyond_uint8(g500):
     n = 300
     edges = np.zeros(n - 1, g500.EDGE_DTYPE)
