@@ -14,7 +14,9 @@
 // row after a push settle in a pass of their own.  The frontier masks are
 // double-buffered by level parity.  Pull or push is chosen per level from
 // edge counts: pull when the new frontier's degree sum exceeds (degree sum of
-// vertices with unvisited lanes) / alpha.
+// vertices with unvisited lanes) / alpha.  On large graphs a push level with
+// a small frontier is sparse: it works on the vertices marked in frontier and
+// touched bitmaps instead of on every vertex (kernel argument SP).
 // Levels come out per root in original-id order through a shared-memory
 // transpose; the whole launch sequence is captured once as a CUDA graph and
 // replayed for every batch.
